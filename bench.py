@@ -1,0 +1,362 @@
+"""Benchmark: particle RK4 steps/s of Emu's evolution path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl emu|reference]
+                    [--workload c2|c3|c5] [--precision fp64|mixed]
+
+A step is one RK4 step (4 stages: deposit, interpolate, -i[H,rho], stage
+update; then wrap, Renormalize and compute_dt on the device) over every
+particle of the workload.  Default workload: C2, the fast-flavor 1D case
+(2 flavors, 1x1x128 cells, 80 Fibonacci directions per cell, 10,240
+particles, FP64).  Inputs are synthetic (seeded initial conditions).
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events
+on the launching stream with an L2 flush (512 MB write) before every step;
+the reported time is the sum of the K step durations, max over ranks.  With
+torchrun (N > 1) every rank runs an independent replica of the workload on
+its own GPU (weak scaling).
+
+--impl reference times the reference's per-particle arithmetic on the host
+cores (oracle/_ref: Emu's generated kernel bodies in the restated AMReX
+loops; the oracle port when _ref is absent) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from emu_b200 import api  # noqa: E402
+from emu_b200 import workloads as W  # noqa: E402
+
+METRIC = "particle RK4 steps/s on 1 B200: mixed vs FP64 at stated err; % of HBM peak"
+
+
+def workload(name, precision):
+    if name == "c2":
+        p = W.c2_fast_flavor_1d()
+        desc = "C2 fast-flavor 1D: 2 flavors, 1x1x128 cells over 64 cm, 80 Fibonacci directions/cell"
+    elif name == "c3":
+        p = W.c3_three_flavor_1d()
+        desc = "C3 3-flavor 1D: 1x1x1024 cells, 378 ring directions/cell"
+    elif name == "c5":
+        p = W.c5_3d()
+        desc = "C5 3-flavor 3D: 64^3 cells x 96 Fibonacci directions"
+    else:
+        raise SystemExit("unknown workload " + name)
+    if precision:
+        p.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
+    return p, desc
+
+
+def algorithmic_bytes_per_particle_step(nf, mixed):
+    """Compulsory HBM bytes per particle per RK4 step of the fused
+    one-pass-per-stage design (S = static fields per pass, F64 = 2 NF^2 FP64
+    flavor reals, Fs = stage-state width, E4 = L, Lbar read + pos, time
+    written): plain 4S + 16 F64 + E4, mixed 4S + 10 F64 + 6 Fs + E4."""
+    F64 = 2 * nf * nf * 8
+    E4 = 48
+    if mixed:
+        S = 48
+        Fs = 2 * nf * nf * 4
+        return 4 * S + 10 * F64 + 6 * Fs + E4
+    S = 72
+    return 4 * S + 16 * F64 + E4
+
+
+def mesh_bytes_per_step(p, nf):
+    ncells = p.ncell[0] * p.ncell[1] * p.ncell[2]
+    return 4 * 2 * ncells * 8 * nf * nf * 8
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for i, n in enumerate(names):
+                if r[5 + i].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(p, recs, budget_s, nthreads):
+    """The reference arithmetic on host cores: run whole steps of the
+    workload until the time budget is spent; particle-steps/s."""
+    from oracle.oracle import Oracle, RefHarness, have_ref
+    kind = "reference" if have_ref(p.nflavors) else "port"
+    o = RefHarness(p) if kind == "reference" else Oracle(p)
+    parts = np.array(recs, copy=True)
+    vmax = o.vvac_max(parts)
+    mesh = o.deposit(parts, nthreads)
+    dt, _ = o.compute_dt(mesh, vmax)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        mesh, _, _ = o.rk_step(parts, dt, nthreads=nthreads)
+        dt, _ = o.compute_dt(mesh, vmax)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or steps >= 100000:
+            break
+    return {"value": len(parts) * steps / el, "unit": "particle-steps/s", "cores": nthreads, "kind": kind,
+            "sample": "%d full RK4 steps of the workload (%d particles), %.1f s" % (steps, len(parts), el)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, local = dist_setup(args)
+    if rank != 0:
+        return
+    p, desc = workload(args.workload, args.precision)
+    recs = api.init_particles(p)
+    nthreads = os.cpu_count() or 1
+    from oracle.oracle import Oracle, RefHarness, have_ref
+    kind = "reference" if have_ref(p.nflavors) else "port"
+    o = RefHarness(p) if kind == "reference" else Oracle(p)
+    # bounded sample: at most ~2 minutes of host time in total
+    parts = np.array(recs, copy=True)
+    vmax = o.vvac_max(parts)
+    mesh = o.deposit(parts, nthreads)
+    dt, _ = o.compute_dt(mesh, vmax)
+    for _ in range(args.warmup):
+        mesh, _, _ = o.rk_step(parts, dt, nthreads=nthreads)
+        dt, _ = o.compute_dt(mesh, vmax)
+    t0 = time.perf_counter()
+    steps = 0
+    for _ in range(args.steps):
+        mesh, _, _ = o.rk_step(parts, dt, nthreads=nthreads)
+        dt, _ = o.compute_dt(mesh, vmax)
+        steps += 1
+        if time.perf_counter() - t0 > 120:
+            break
+    el = time.perf_counter() - t0
+    value = len(parts) * steps / el
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+           "n_gpus": ws, "steps": steps, "warmup": args.warmup, "ms_per_step": el / steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic",
+           "config": {"workload": desc, "particles": len(parts), "nflavors": p.nflavors,
+                      "cells": list(p.ncell)},
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": nthreads, "kind": kind,
+                            "sample": "%d RK4 steps of the full workload" % steps},
+           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def run_emu(args):
+    import torch
+    ws, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    p, desc = workload(args.workload, args.precision)
+    mixed = p.precision == api.PREC_MIXED
+    nf = p.nflavors
+    recs = api.init_particles(p)
+    n = recs.shape[0]
+    stream = torch.cuda.Stream()
+    ctx = api.Context(p)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load_particles(recs)
+    total_steps = args.warmup + args.steps + args.profile_steps + 8
+    ctx.evolve_begin(0.0, float("inf"), total_steps)
+    flush_bytes = 512 << 20
+    flush = torch.zeros(flush_bytes // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        ctx.flush_l2(flush.data_ptr(), flush_bytes)
+        ctx.evolve_steps(1)
+    ctx.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    sampler.start()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for i in range(args.steps):
+        ctx.flush_l2(flush.data_ptr(), flush_bytes)
+        evs[i][0].record(stream)
+        ctx.evolve_steps(1)
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    info = ctx.evolve_end()
+    if info.status != 0:
+        raise SystemExit("device status %d during the benchmark: %s" % (info.status, api.last_error(ctx.h)))
+    value = n * args.steps * ws / (total_ms * 1e-3)
+
+    # roofline of the stage kernel: per-kernel CUDA events on the stream
+    ctx.evolve_begin(0.0, float("inf"), args.profile_steps + 2)
+    kms = []
+    for _ in range(args.profile_steps):
+        ctx.flush_l2(flush.data_ptr(), flush_bytes)
+        kms.append(ctx.profile_step())
+    kms = np.array(kms)
+    stage_idx = [1, 3, 5, 7] if mixed else [0, 1, 2, 3]
+    stage_ms = float(kms[:, stage_idx].mean())
+    per_pstep = algorithmic_bytes_per_particle_step(nf, mixed)
+    bytes_per_launch = (per_pstep * n + mesh_bytes_per_step(p, nf)) / 4.0
+    peak, peak_kind = load_peaks()
+    achieved = bytes_per_launch / (stage_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (args.workload, "mixed" if mixed else "fp64"))
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    # end to end through the C ABI with host buffers: upload the state from
+    # pinned memory, one device step, download the state
+    e2e = None
+    if not args.no_e2e:
+        pin_in = torch.from_numpy(recs).pin_memory()
+        pin_out = torch.empty_like(pin_in).pin_memory()
+        ne = min(args.steps, args.e2e_steps)
+        torch.cuda.synchronize()
+        e0 = time.perf_counter()
+        for _ in range(ne):
+            ctx.load_particles_ptr(pin_in.data_ptr(), n)
+            ctx.evolve_begin(0.0, float("inf"), 1)
+            ctx.evolve_steps(1)
+            ctx.get_particles_ptr(pin_out.data_ptr(), n)
+        el = time.perf_counter() - e0
+        t = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        bytes_rec = n * api.nreal(nf) * 8
+        e2e = {"value": n * ne * ws / float(t.item()), "unit": "particle-steps/s",
+               "h2d_bytes_per_step": bytes_rec, "d2h_bytes_per_step": bytes_rec,
+               "note": "per step: emu_load_particles from pinned host memory, emu_evolve_begin "
+                       "(deposit + compute_dt), one device step, emu_get_particles to pinned host memory"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(p, recs, args.cpu_budget, os.cpu_count() or 1)
+
+    kernels_per_step = 9 if mixed else 5
+    resorts = (args.steps // p.resort_interval) if p.resort_interval > 0 else 0
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "particle-steps/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "mixed(f32/i64/f64)" if mixed else "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "particles": n, "nflavors": nf, "cells": list(p.ncell),
+                   "precision": "mixed" if mixed else "fp64", "integrator": "RK4",
+                   "l2": "flushed (512 MB write) before every timed step",
+                   "parallelism": "replica per GPU" if ws > 1 else "1 GPU",
+                   "resort_interval": p.resort_interval},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "k_rk4_stage%s<%d>" % ("_mixed" if mixed else "", nf),
+                     "kernel_ms": stage_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "peak_source": peak_kind},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "gpu_launches": args.steps * kernels_per_step + 2 * resorts + args.steps,
+        "clocks": clocks,
+        "wall_s": wall,
+        "kernel_ms_per_step": [float(x) for x in kms.mean(axis=0)],
+    }
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="emu", choices=["emu", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"])
+    ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_emu(args)
+
+
+if __name__ == "__main__":
+    main()

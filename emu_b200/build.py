@@ -1,0 +1,78 @@
+"""Build the CUDA library libemu_b200.so in-tree (sm_100a).
+
+    python -m emu_b200.build [--force] [--verbose-ptxas]
+
+Objects go to emu_b200/_build/, the shared library to emu_b200/libemu_b200.so
+(next to this file, so it travels with the source tree).  nvcc cross-compiles
+without a GPU.
+"""
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libemu_b200.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
+
+SOURCES = ["emu_kernels.cu", "emu_capi.cu", "emu_host.cpp", "emu_init.cpp"]
+HEADERS = ["emu_device.cuh", "emu_kernels.cuh", "emu_host.h"]
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _compile(src, verbose_ptxas):
+    path = os.path.join(CSRC, src)
+    obj = os.path.join(OBJ, src + ".o")
+    deps = [path] + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "emu_b200.h")]
+    if not _stale(obj, deps):
+        return obj, ""
+    cmd = [NVCC] + ARCH + COMMON + ["-c", path, "-o", obj]
+    if src.endswith(".cu"):
+        cmd += ["--extended-lambda", "-Xptxas", "-warn-spills"]
+        if verbose_ptxas:
+            cmd += ["-Xptxas", "-v"]
+    else:
+        cmd += ["-x", "c++"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
+    return obj, r.stderr
+
+
+def build(force=False, verbose_ptxas=False, quiet=True):
+    os.makedirs(OBJ, exist_ok=True)
+    if force:
+        for s in SOURCES:
+            o = os.path.join(OBJ, s + ".o")
+            if os.path.exists(o):
+                os.remove(o)
+    with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(lambda s: _compile(s, verbose_ptxas), SOURCES))
+    objs = [r[0] for r in results]
+    logs = "".join(r[1] for r in results)
+    if logs and not quiet:
+        sys.stderr.write(logs)
+    if force or _stale(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    return LIB, logs
+
+
+if __name__ == "__main__":
+    lib, logs = build(force="--force" in sys.argv, verbose_ptxas="--verbose-ptxas" in sys.argv, quiet=False)
+    print(lib)

@@ -1,0 +1,848 @@
+// emu_capi.cu -- the C ABI (include/emu_b200.h): device context, particle
+// upload/download with on-device cell sorting, the step drivers (fused RK4,
+// unfused Butcher tableau, mixed precision) and the CUDA-graph step loop.
+#include "emu_b200.h"
+#include "emu_host.h"
+#include "emu_kernels.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using emu::DevParams;
+using emu::DevState;
+using emu::StepCtl;
+
+struct emu_context {
+    emu_params prm;
+    DevParams P;
+    int nf = 2, NH = 4, NS = 8, ND = 32, nreal = 23;
+    bool mixed = false;
+    cudaStream_t stream = nullptr;      // where work is launched
+    cudaStream_t own = nullptr;         // the context's own stream
+    cudaStream_t cap_stream = nullptr;  // private stream used for graph capture
+    DevState S[2];                      // persistent particle arrays, double-buffered for re-sorts
+    int cur = 0;                        // which of S[] is current
+    void* pblock[2] = {nullptr, nullptr};
+    void* tblock = nullptr;             // transient per-step arrays
+    long long cap = 0;
+    double* mesh[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long* qmesh[2] = {nullptr, nullptr};
+    float* gmesh = nullptr;
+    double* fmesh_tmp = nullptr;        // FP64 cell-major copy (mixed API calls)
+    double* planes = nullptr;           // ncomp x ncells output staging
+    StepCtl* ctl = nullptr;
+    StepCtl* ctl_host = nullptr;        // pinned
+    double* aos = nullptr;              // AoS staging (n x nreal)
+    long long aos_cap = 0;
+    unsigned *keys = nullptr, *keys2 = nullptr, *idx = nullptr, *idx2 = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int cur_mesh = 0;
+    bool fused_ready = false;
+    bool loaded = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int steps_since_sort = 0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_host_err;
+
+int fail(emu_context* c, int code, const std::string& msg)
+{
+    if (c) c->err = msg; else g_host_err = msg;
+    return code;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, EMU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+int check_launch(emu_context* ctx, const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return EMU_OK;
+}
+
+int widths(int ord) { return ord >= 2 ? 3 : (ord == 1 ? 2 : 1); }
+
+// DevParams from the run parameters (geometry as AMReX computes it:
+// CellSize = L/n, InvCellSize = 1/CellSize)
+void make_devparams(const emu_params& p, DevParams& P)
+{
+    std::memset(&P, 0, sizeof(P));
+    P.nf = p.nflavors;
+    double L[3] = {p.Lx, p.Ly, p.Lz};
+    double dx[3];
+    for (int d = 0; d < 3; d++) {
+        P.n[d] = p.ncell[d];
+        P.ord[d] = p.ncell[d] > 1 ? p.shape_order : 0;
+        P.w[d] = widths(P.ord[d]);
+        P.L[d] = L[d];
+        dx[d] = L[d] / (double)p.ncell[d];
+        P.dxi[d] = 1.0 / dx[d];
+    }
+    P.ncells = (long long)p.ncell[0] * p.ncell[1] * p.ncell[2];
+    const double inv_cell_volume = P.dxi[0] * P.dxi[1] * P.dxi[2];
+    P.cell_volume = dx[0] * dx[1] * dx[2];
+    P.GF = emu_host::gf();
+    P.sqrt2GF = std::sqrt(2.) * P.GF;
+    P.sqrt2GF_inv_vol = P.sqrt2GF * inv_cell_volume;
+    P.matter = p.rho_in * p.Ye_in / emu::kMp / inv_cell_volume;
+    P.rho = p.rho_in;
+    P.Ye = p.Ye_in;
+    P.c4 = emu_host::c4();
+    P.inv_hbar = 1.0 / emu::kHbar;
+    P.maxError = p.maxError;
+    P.cfl_factor = p.cfl_factor;
+    P.flavor_cfl_factor = p.flavor_cfl_factor;
+    P.max_adaptive_speedup = p.max_adaptive_speedup;
+    P.dt_translation = 0.0;
+    if (p.cfl_factor > 0.0) P.dt_translation = std::min(std::min(dx[0], dx[1]), dx[2]) / emu::kC * p.cfl_factor;
+    double m2[2][9];
+    emu_host::vacuum_m2(p, m2);
+    for (int s = 0; s < 2; s++)
+        for (int e = 0; e < 9; e++) P.M2[s][e] = m2[s][e];
+    P.q_scale[0] = P.q_scale[1] = 1.0;
+    P.q_unscale[0] = P.q_unscale[1] = 1.0;
+}
+
+template <class T>
+T* carve(char*& ptr, long long count)
+{
+    T* r = reinterpret_cast<T*>(ptr);
+    size_t bytes = ((size_t)count * sizeof(T) + 255) & ~(size_t)255;
+    ptr += bytes;
+    return r;
+}
+
+size_t persistent_bytes(int NS, bool mixed, long long cap)
+{
+    size_t per = (size_t)(16 + NS) * 8 + 8;
+    if (mixed) per += 5 * 4;
+    return per * cap + 64 * 256;
+}
+
+size_t transient_bytes(int NS, bool mixed, long long cap)
+{
+    if (mixed) return (size_t)2 * NS * 4 * cap + 4 * 256;
+    return (size_t)2 * NS * 8 * cap + 4 * 256;
+}
+
+void assign_persistent(DevState& S, void* block, int NS, bool mixed, long long cap)
+{
+    char* p = static_cast<char*>(block);
+    for (int d = 0; d < 3; d++) S.pos[d] = carve<double>(p, cap);
+    S.time = carve<double>(p, cap);
+    for (int d = 0; d < 4; d++) S.pup[d] = carve<double>(p, cap);
+    for (int s = 0; s < 2; s++) S.Nn[s] = carve<double>(p, cap);
+    for (int s = 0; s < 2; s++) S.Ll[s] = carve<double>(p, cap);
+    for (int d = 0; d < 3; d++) S.vhat[d] = carve<double>(p, cap);
+    S.vscale = carve<double>(p, cap);
+    S.f0 = carve<double>(p, (long long)NS * cap);
+    S.id = carve<long long>(p, cap);
+    if (mixed) {
+        for (int d = 0; d < 3; d++) S.vhat32[d] = carve<float>(p, cap);
+        for (int s = 0; s < 2; s++) S.N32[s] = carve<float>(p, cap);
+    }
+    S.cap = cap;
+}
+
+void assign_transient(DevState& S, void* block, int NS, bool mixed, long long cap)
+{
+    char* p = static_cast<char*>(block);
+    if (mixed) {
+        S.k32 = carve<float>(p, (long long)NS * cap);
+        S.ksum32 = carve<float>(p, (long long)NS * cap);
+        S.fs = S.acc = nullptr;
+    } else {
+        S.fs = carve<double>(p, (long long)NS * cap);
+        S.acc = carve<double>(p, (long long)NS * cap);
+        S.k32 = S.ksum32 = nullptr;
+    }
+}
+
+void free_graphs(emu_context* c)
+{
+    for (int i = 0; i < 2; i++)
+        if (c->graph[i]) {
+            cudaGraphExecDestroy(c->graph[i]);
+            c->graph[i] = nullptr;
+        }
+}
+
+int ensure_capacity(emu_context* ctx, long long n)
+{
+    if (n <= ctx->cap && ctx->pblock[0]) return EMU_OK;
+    free_graphs(ctx);
+    for (int i = 0; i < 2; i++)
+        if (ctx->pblock[i]) cudaFree(ctx->pblock[i]);
+    if (ctx->tblock) cudaFree(ctx->tblock);
+    if (ctx->S[0].kgen) cudaFree(ctx->S[0].kgen);
+    if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
+    if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
+    ctx->pblock[0] = ctx->pblock[1] = ctx->tblock = nullptr;
+    ctx->keys = ctx->keys2 = ctx->idx = ctx->idx2 = nullptr;
+    ctx->sort_tmp = nullptr;
+    ctx->S[0].kgen = ctx->S[1].kgen = nullptr;
+    const long long cap = std::max<long long>(n, 1);
+    for (int i = 0; i < 2; i++) {
+        CU(cudaMalloc(&ctx->pblock[i], persistent_bytes(ctx->NS, ctx->mixed, cap)));
+        ctx->S[i] = DevState();
+        assign_persistent(ctx->S[i], ctx->pblock[i], ctx->NS, ctx->mixed, cap);
+    }
+    CU(cudaMalloc(&ctx->tblock, transient_bytes(ctx->NS, ctx->mixed, cap)));
+    for (int i = 0; i < 2; i++) assign_transient(ctx->S[i], ctx->tblock, ctx->NS, ctx->mixed, cap);
+    CU(cudaMalloc(&ctx->keys, sizeof(unsigned) * cap));
+    CU(cudaMalloc(&ctx->keys2, sizeof(unsigned) * cap));
+    CU(cudaMalloc(&ctx->idx, sizeof(unsigned) * cap));
+    CU(cudaMalloc(&ctx->idx2, sizeof(unsigned) * cap));
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, ctx->keys, ctx->keys2, ctx->idx, ctx->idx2, (int)cap);
+    ctx->sort_tmp_bytes = tb + 256;
+    CU(cudaMalloc(&ctx->sort_tmp, ctx->sort_tmp_bytes));
+    ctx->cap = cap;
+    return EMU_OK;
+}
+
+int ensure_aos(emu_context* ctx, long long n)
+{
+    if (n <= ctx->aos_cap && ctx->aos) return EMU_OK;
+    if (ctx->aos) cudaFree(ctx->aos);
+    ctx->aos = nullptr;
+    CU(cudaMalloc(&ctx->aos, sizeof(double) * (size_t)std::max<long long>(n, 1) * ctx->nreal));
+    ctx->aos_cap = std::max<long long>(n, 1);
+    return EMU_OK;
+}
+
+int key_bits(long long ncells)
+{
+    int b = 1;
+    while ((1ll << b) < ncells) b++;
+    return b;
+}
+
+// device radix sort of (keys, idx) -> idx2 holds the permutation
+int sort_perm(emu_context* ctx, long long n)
+{
+    size_t tb = ctx->sort_tmp_bytes;
+    CU(cub::DeviceRadixSort::SortPairs(ctx->sort_tmp, tb, ctx->keys, ctx->keys2, ctx->idx, ctx->idx2, (int)n, 0,
+                                       key_bits(ctx->P.ncells), ctx->stream));
+    return EMU_OK;
+}
+
+int sync_ctl(emu_context* ctx)
+{
+    CU(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
+int status_of(emu_context* ctx, int64_t* bad)
+{
+    const StepCtl& h = *ctx->ctl_host;
+    if (bad) *bad = (h.bad == LLONG_MAX) ? -1 : (int64_t)h.bad;
+    if (h.status) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "device status 0x%x (first particle %lld): %s%s%s%s", h.status,
+                      h.bad == LLONG_MAX ? -1ll : (long long)h.bad,
+                      (h.status & EMU_ERR_TRACE) ? "trace error exceeds 100*maxError; " : "",
+                      (h.status & EMU_ERR_NEGDIAG) ? "negative diagonal below -100*maxError; " : "",
+                      (h.status & EMU_ERR_LENGTH) ? "flavor vector length error exceeds 100*maxError; " : "",
+                      (h.status & EMU_ERR_DT) ? "timestep selection failed (no limiter); " : "");
+        ctx->err = buf;
+    }
+    return h.status;
+}
+
+// ---- mesh helpers ----------------------------------------------------------
+long long mesh_elems(const emu_context* c) { return c->P.ncells * c->ND; }
+
+int zero_mesh(emu_context* ctx, int i)
+{
+    if (ctx->mixed) CU(cudaMemsetAsync(ctx->qmesh[i], 0, sizeof(long long) * mesh_elems(ctx), ctx->stream));
+    else CU(cudaMemsetAsync(ctx->mesh[i], 0, sizeof(double) * mesh_elems(ctx), ctx->stream));
+    return EMU_OK;
+}
+
+// deposit of the current state into mesh slot 0 and a clean slot 1: the
+// state the fused step loop expects at a step boundary
+int deposit_current(emu_context* ctx)
+{
+    DevState& S = ctx->S[ctx->cur];
+    int r;
+    if ((r = zero_mesh(ctx, 0))) return r;
+    if ((r = zero_mesh(ctx, 1))) return r;
+    if (ctx->mixed) emu::launch_deposit_q(ctx->nf, ctx->P, S, S.f0, ctx->qmesh[0], ctx->stream);
+    else emu::launch_deposit(ctx->nf, ctx->P, S, S.f0, ctx->mesh[0], ctx->stream);
+    if ((r = check_launch(ctx, "deposit"))) return r;
+    ctx->cur_mesh = 0;
+    ctx->fused_ready = true;
+    return EMU_OK;
+}
+
+// ---- step bodies -----------------------------------------------------------
+// fused FP64 RK4: stage s reads mesh[s-1], deposits mesh[s%4], zeros mesh[(s+1)%4]
+int enqueue_rk4_fp64(emu_context* ctx, cudaStream_t st, bool with_dt)
+{
+    const DevState& S = ctx->S[ctx->cur];
+    for (int s = 1; s <= 4; s++)
+        emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4], ctx->mesh[(s + 1) % 4],
+                              mesh_elems(ctx), ctx->ctl, st);
+    if (with_dt) emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[3], ctx->ctl, emu::DT_ADVANCE, st);
+    return check_launch(ctx, "rk4 stage");
+}
+
+// mixed RK4: finalize(q[a] -> g, zero q[b]); stage deposits into q[b]; swap
+int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt)
+{
+    const DevState& S = ctx->S[ctx->cur];
+    int a = 0;
+    for (int s = 1; s <= 4; s++) {
+        const int b = 1 - a;
+        emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, st);
+        emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->ctl, st);
+        a = b;
+    }
+    // M_4 sits in q[1] until the next step's first finalize zeroes it
+    if (with_dt) emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[1], ctx->ctl, emu::DT_ADVANCE, st);
+    return check_launch(ctx, "rk4 mixed stage");
+}
+
+// Butcher tableau of the integrator (TimeIntegrator: FE, trapezoid, SSPRK3, RK4)
+int tableau(const emu_params& p, int& ns, double A[4][4], double b[4])
+{
+    std::memset(A, 0, sizeof(double) * 16);
+    std::memset(b, 0, sizeof(double) * 4);
+    if (p.integration_type == 0) {
+        ns = 1; b[0] = 1.0;
+    } else if (p.rk_type == 2) {
+        ns = 2; A[1][0] = 1.0; b[0] = 0.5; b[1] = 0.5;
+    } else if (p.rk_type == 3) {
+        ns = 3; A[1][0] = 1.0; A[2][0] = 0.25; A[2][1] = 0.25;
+        b[0] = 1. / 6.; b[1] = 1. / 6.; b[2] = 2. / 3.;
+    } else if (p.rk_type == 4) {
+        ns = 4; A[1][0] = 0.5; A[2][1] = 0.5; A[3][2] = 1.0;
+        b[0] = 1. / 6.; b[1] = 1. / 3.; b[2] = 1. / 3.; b[3] = 1. / 6.;
+    } else {
+        return EMU_ERR_ARG;
+    }
+    return EMU_OK;
+}
+
+// unfused explicit RK step with host dt (FP64 only)
+int step_generic(emu_context* ctx, double dt)
+{
+    int ns;
+    double A[4][4], b[4];
+    if (tableau(ctx->prm, ns, A, b)) return fail(ctx, EMU_ERR_ARG, "unsupported integrator");
+    DevState& S = ctx->S[ctx->cur];
+    const long long kstride = (long long)ctx->NS * ctx->cap;
+    if (!S.kgen) {
+        CU(cudaMalloc(&ctx->S[0].kgen, sizeof(double) * 4 * kstride));
+        ctx->S[1].kgen = ctx->S[0].kgen;
+    }
+    int r;
+    for (int i = 0; i < ns; i++) {
+        const double* Y = S.f0;
+        if (i > 0) {
+            double coef[3];
+            for (int j = 0; j < i; j++) coef[j] = dt * A[i][j];
+            emu::launch_stage_state(ctx->nf, S, S.kgen, i, coef, S.fs, ctx->stream);
+            Y = S.fs;
+        }
+        if ((r = zero_mesh(ctx, 0))) return r;
+        emu::launch_deposit(ctx->nf, ctx->P, S, Y, ctx->mesh[0], ctx->stream);
+        emu::launch_rhs(ctx->nf, ctx->P, S, Y, ctx->mesh[0], S.kgen + i * kstride, ctx->stream);
+    }
+    double w[4];
+    for (int i = 0; i < ns; i++) w[i] = dt * b[i];
+    emu::launch_combine(ctx->nf, ctx->P, S, S.kgen, ns, w, ctx->ctl, ctx->stream);
+    if ((r = check_launch(ctx, "generic step"))) return r;
+    ctx->cur_mesh = 0;
+    ctx->fused_ready = false;
+    return EMU_OK;
+}
+
+int resort(emu_context* ctx)
+{
+    DevState& src = ctx->S[ctx->cur];
+    DevState& dst = ctx->S[1 - ctx->cur];
+    dst.n = src.n;
+    emu::launch_state_keys(ctx->P, src, ctx->keys, ctx->idx, ctx->stream);
+    int r;
+    if ((r = sort_perm(ctx, src.n))) return r;
+    emu::launch_gather_state(ctx->nf, ctx->mixed, src, dst, ctx->idx2, ctx->stream);
+    if ((r = check_launch(ctx, "resort"))) return r;
+    ctx->cur = 1 - ctx->cur;
+    ctx->steps_since_sort = 0;
+    // the deposited meshes are order independent; stage 1 of the next step
+    // reads the same mesh as before the re-sort
+    return EMU_OK;
+}
+
+int enqueue_step_body(emu_context* ctx, cudaStream_t st)
+{
+    return ctx->mixed ? enqueue_rk4_mixed(ctx, st, true) : enqueue_rk4_fp64(ctx, st, true);
+}
+
+int build_graph(emu_context* ctx)
+{
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int r = enqueue_step_body(ctx, ctx->cap_stream);
+    cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    ctx->graph[ctx->cur] = ex;
+    return EMU_OK;
+}
+
+bool rk4_fused(const emu_context* ctx)
+{
+    return ctx->prm.integration_type == 1 && ctx->prm.rk_type == 4 && (ctx->mixed || ctx->prm.fused);
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int emu_abi_version(void) { return EMU_B200_ABI_VERSION; }
+int emu_nattribs(int nf) { return 8 + 2 * (2 + nf * nf); }
+int emu_nreal(int nf) { return 3 + emu_nattribs(nf); }
+int emu_ncomp(int nf) { return 3 + 8 * nf * nf; }
+
+int emu_last_error(const emu_context* ctx, char* buf, size_t len)
+{
+    const std::string& s = ctx ? ctx->err : g_host_err;
+    if (buf && len) {
+        std::strncpy(buf, s.c_str(), len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)s.size();
+}
+
+int emu_create(const emu_params* p, emu_context** out)
+{
+    emu_context* ctx = nullptr;
+    if (!p || !out) return fail(nullptr, EMU_ERR_ARG, "emu_create: null argument");
+    *out = nullptr;
+    std::string why;
+    if (!emu_host::validate(*p, why)) return fail(nullptr, EMU_ERR_ARG, "emu_create: " + why);
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(nullptr, EMU_ERR_CUDA, std::string("emu_create: no CUDA device: ") + cudaGetErrorString(e));
+    ctx = new emu_context();
+    ctx->prm = *p;
+    ctx->nf = p->nflavors;
+    ctx->NH = ctx->nf * ctx->nf;
+    ctx->NS = 2 * ctx->NH;
+    ctx->ND = 8 * ctx->NH;
+    ctx->nreal = emu_nreal(ctx->nf);
+    ctx->mixed = p->precision == EMU_PREC_MIXED;
+    make_devparams(*p, ctx->P);
+    int r = EMU_OK;
+    auto bail = [&](int code) {
+        g_host_err = ctx->err;
+        emu_destroy(ctx);
+        return code;
+    };
+    e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return bail(EMU_ERR_CUDA); }
+    e = cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return bail(EMU_ERR_CUDA); }
+    ctx->stream = ctx->own;
+    const size_t me = (size_t)mesh_elems(ctx);
+    if (ctx->mixed) {
+        for (int i = 0; i < 2 && !r; i++)
+            if (cudaMalloc(&ctx->qmesh[i], sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+        if (!r && cudaMalloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * 4 * ctx->NH) != cudaSuccess)
+            r = EMU_ERR_NOMEM;
+    } else {
+        for (int i = 0; i < 4 && !r; i++)
+            if (cudaMalloc(&ctx->mesh[i], sizeof(double) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+    }
+    if (!r && cudaMalloc(&ctx->planes, sizeof(double) * ctx->P.ncells * emu_ncomp(ctx->nf)) != cudaSuccess)
+        r = EMU_ERR_NOMEM;
+    if (!r && cudaMalloc(&ctx->ctl, sizeof(StepCtl)) != cudaSuccess) r = EMU_ERR_NOMEM;
+    if (!r && cudaMallocHost(&ctx->ctl_host, sizeof(StepCtl)) != cudaSuccess) r = EMU_ERR_NOMEM;
+    if (r) {
+        ctx->err = "emu_create: device allocation failed";
+        return bail(r);
+    }
+    cudaMemset(ctx->ctl, 0, sizeof(StepCtl));
+    std::memset(ctx->ctl_host, 0, sizeof(StepCtl));
+    for (int i = 0; i < 4; i++)
+        if (ctx->mesh[i]) cudaMemset(ctx->mesh[i], 0, sizeof(double) * me);
+    for (int i = 0; i < 2; i++)
+        if (ctx->qmesh[i]) cudaMemset(ctx->qmesh[i], 0, sizeof(long long) * me);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        ctx->err = "emu_create: device initialisation failed";
+        return bail(EMU_ERR_CUDA);
+    }
+    *out = ctx;
+    return EMU_OK;
+}
+
+void emu_destroy(emu_context* ctx)
+{
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_graphs(ctx);
+    for (int i = 0; i < 2; i++) if (ctx->pblock[i]) cudaFree(ctx->pblock[i]);
+    if (ctx->tblock) cudaFree(ctx->tblock);
+    if (ctx->S[0].kgen) cudaFree(ctx->S[0].kgen);
+    for (int i = 0; i < 4; i++) if (ctx->mesh[i]) cudaFree(ctx->mesh[i]);
+    for (int i = 0; i < 2; i++) if (ctx->qmesh[i]) cudaFree(ctx->qmesh[i]);
+    if (ctx->gmesh) cudaFree(ctx->gmesh);
+    if (ctx->fmesh_tmp) cudaFree(ctx->fmesh_tmp);
+    if (ctx->planes) cudaFree(ctx->planes);
+    if (ctx->ctl) cudaFree(ctx->ctl);
+    if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+    if (ctx->aos) cudaFree(ctx->aos);
+    if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
+    if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    delete ctx;
+}
+
+int emu_set_stream(emu_context* ctx, void* s)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = s ? static_cast<cudaStream_t>(s) : ctx->own;
+    return EMU_OK;
+}
+
+int emu_synchronize(emu_context* ctx)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
+int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
+{
+    if (!ctx || (n > 0 && !records) || n < 0) return fail(ctx, EMU_ERR_ARG, "emu_load_particles: bad arguments");
+    if (n > (int64_t)INT_MAX) return fail(ctx, EMU_ERR_LIMIT, "emu_load_particles: more than 2^31-1 particles");
+    if (n == 0) return fail(ctx, EMU_ERR_ARG, "emu_load_particles: no particles");
+    int r;
+    if ((r = ensure_capacity(ctx, n))) return r;
+    if ((r = ensure_aos(ctx, n))) return r;
+    CU(cudaMemcpyAsync(ctx->aos, records, sizeof(double) * (size_t)n * ctx->nreal, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    // host-side scalars derived from the particles: Vvac_max (Init.cpp:657-660)
+    // and, for the mixed path, the fixed-point scales
+    double vvac = 0.0;
+    emu_vvac_max(&ctx->prm, records, n, &vvac);
+    ctx->P.vvac_max = vvac;
+    if (ctx->mixed) {
+        std::string why;
+        if (!emu_host::fixed_point_scales(ctx->prm, records, n, ctx->P.q_scale, ctx->P.q_unscale, why))
+            return fail(ctx, EMU_ERR_LIMIT, "emu_load_particles: " + why);
+    }
+    emu::launch_cell_keys(ctx->P, ctx->aos, ctx->nreal, n, ctx->keys, ctx->idx, ctx->stream);
+    if ((r = sort_perm(ctx, n))) return r;
+    ctx->cur = 0;
+    DevState& S = ctx->S[0];
+    S.n = n;
+    ctx->S[1].n = n;
+    emu::launch_pack(ctx->nf, ctx->P, ctx->aos, ctx->idx2, n, S, ctx->stream);
+    if (ctx->mixed) emu::launch_mixed_shadow(ctx->nf, S, ctx->stream);
+    if ((r = check_launch(ctx, "pack"))) return r;
+    free_graphs(ctx);   // kernel arguments (P, S) changed
+    ctx->loaded = true;
+    ctx->steps_since_sort = 0;
+    if ((r = deposit_current(ctx))) return r;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
+int emu_get_particles(emu_context* ctx, double* records, int64_t n)
+{
+    if (!ctx || !records) return fail(ctx, EMU_ERR_ARG, "emu_get_particles: bad arguments");
+    if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_get_particles: no particles loaded");
+    const DevState& S = ctx->S[ctx->cur];
+    if (n < S.n) return fail(ctx, EMU_ERR_ARG, "emu_get_particles: output too small");
+    int r;
+    if ((r = ensure_aos(ctx, S.n))) return r;
+    emu::launch_unpack(ctx->nf, S, ctx->aos, ctx->stream);
+    if ((r = check_launch(ctx, "unpack"))) return r;
+    CU(cudaMemcpyAsync(records, ctx->aos, sizeof(double) * (size_t)S.n * ctx->nreal, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
+int emu_num_particles(const emu_context* ctx, int64_t* n)
+{
+    if (!ctx || !n) return EMU_ERR_ARG;
+    *n = ctx->loaded ? ctx->S[ctx->cur].n : 0;
+    return EMU_OK;
+}
+
+int emu_deposit(emu_context* ctx)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_deposit: no particles loaded");
+    int r = deposit_current(ctx);
+    if (r) return r;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
+int emu_get_mesh(emu_context* ctx, double* out)
+{
+    if (!ctx || !out) return fail(ctx, EMU_ERR_ARG, "emu_get_mesh: bad arguments");
+    const long long nc = ctx->P.ncells;
+    if (ctx->mixed) emu::launch_mesh_out_q(ctx->nf, ctx->P, ctx->qmesh[ctx->cur_mesh], ctx->planes, ctx->stream);
+    else emu::launch_mesh_out(ctx->nf, ctx->P, ctx->mesh[ctx->cur_mesh], ctx->planes, ctx->stream);
+    int r;
+    if ((r = check_launch(ctx, "mesh out"))) return r;
+    CU(cudaMemcpyAsync(out + 3 * nc, ctx->planes + 3 * nc, sizeof(double) * nc * ctx->ND, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (long long c = 0; c < nc; c++) {
+        out[c] = ctx->prm.rho_in;
+        out[nc + c] = ctx->prm.T_in;
+        out[2 * nc + c] = ctx->prm.Ye_in;
+    }
+    return EMU_OK;
+}
+
+int emu_interpolate_rhs(emu_context* ctx, double* rhs_records)
+{
+    if (!ctx || !rhs_records) return fail(ctx, EMU_ERR_ARG, "emu_interpolate_rhs: bad arguments");
+    if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_interpolate_rhs: no particles loaded");
+    DevState& S = ctx->S[ctx->cur];
+    const long long kstride = (long long)ctx->NS * ctx->cap;
+    if (!S.kgen) {
+        CU(cudaMalloc(&ctx->S[0].kgen, sizeof(double) * 4 * kstride));
+        ctx->S[1].kgen = ctx->S[0].kgen;
+    }
+    const double* mesh = nullptr;
+    if (ctx->mixed) {
+        // the FP64 interpolation of the fixed-point mesh
+        if (!ctx->fmesh_tmp) CU(cudaMalloc(&ctx->fmesh_tmp, sizeof(double) * mesh_elems(ctx)));
+        emu::launch_q_to_f64(ctx->nf, ctx->P, ctx->qmesh[ctx->cur_mesh], ctx->fmesh_tmp, ctx->stream);
+        mesh = ctx->fmesh_tmp;
+    } else {
+        mesh = ctx->mesh[ctx->cur_mesh];
+    }
+    emu::launch_rhs(ctx->nf, ctx->P, S, S.f0, mesh, S.kgen, ctx->stream);
+    int r;
+    if ((r = ensure_aos(ctx, S.n))) return r;
+    emu::launch_unpack_rhs(ctx->nf, S, S.kgen, ctx->aos, ctx->stream);
+    if ((r = check_launch(ctx, "rhs"))) return r;
+    CU(cudaMemcpyAsync(rhs_records, ctx->aos, sizeof(double) * (size_t)S.n * ctx->nreal, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
+int emu_renormalize(emu_context* ctx, int64_t* bad)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_renormalize: no particles loaded");
+    emu::launch_ctl_set(ctx->ctl, 0.0, 0.0, 0.0, 1, 1, ctx->stream);
+    emu::launch_renorm(ctx->nf, ctx->P, ctx->S[ctx->cur], ctx->ctl, ctx->stream);
+    int r;
+    if ((r = check_launch(ctx, "renormalize"))) return r;
+    ctx->fused_ready = false;
+    if ((r = sync_ctl(ctx))) return r;
+    return status_of(ctx, bad);
+}
+
+int emu_compute_dt(emu_context* ctx, double* dt)
+{
+    if (!ctx || !dt) return EMU_ERR_ARG;
+    emu::launch_ctl_set(ctx->ctl, 0.0, 0.0, 0.0, 1, 1, ctx->stream);
+    if (ctx->mixed) emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[ctx->cur_mesh], ctx->ctl, emu::DT_QUERY, ctx->stream);
+    else emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[ctx->cur_mesh], ctx->ctl, emu::DT_QUERY, ctx->stream);
+    int r;
+    if ((r = check_launch(ctx, "compute_dt"))) return r;
+    if ((r = sync_ctl(ctx))) return r;
+    *dt = ctx->ctl_host->dt;
+    return status_of(ctx, nullptr);
+}
+
+int emu_step(emu_context* ctx, double dt, int64_t* bad)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_step: no particles loaded");
+    if (!(dt >= 0.0) || !std::isfinite(dt)) return fail(ctx, EMU_ERR_ARG, "emu_step: dt must be finite and >= 0");
+    int r;
+    emu::launch_ctl_set(ctx->ctl, dt, 0.0, INFINITY, 1, 1, ctx->stream);
+    if (rk4_fused(ctx)) {
+        if (!ctx->fused_ready && (r = deposit_current(ctx))) return r;
+        r = ctx->mixed ? enqueue_rk4_mixed(ctx, ctx->stream, false) : enqueue_rk4_fp64(ctx, ctx->stream, false);
+        if (r) return r;
+        ctx->cur_mesh = ctx->mixed ? 1 : 3;
+        ctx->fused_ready = true;
+    } else {
+        if (ctx->mixed) return fail(ctx, EMU_ERR_ARG, "emu_step: the mixed path integrates with RK4 only");
+        if ((r = step_generic(ctx, dt))) return r;
+    }
+    if (++ctx->steps_since_sort >= ctx->prm.resort_interval && ctx->prm.resort_interval > 0)
+        if ((r = resort(ctx))) return r;
+    if ((r = sync_ctl(ctx))) return r;
+    return status_of(ctx, bad);
+}
+
+int emu_evolve_begin(emu_context* ctx, double start_time, double end_time, int max_steps)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_evolve: no particles loaded");
+    if (!rk4_fused(ctx)) return fail(ctx, EMU_ERR_ARG, "emu_evolve: device-resident loop requires fused RK4");
+    int r;
+    if (!ctx->fused_ready && (r = deposit_current(ctx))) return r;
+    emu::launch_ctl_set(ctx->ctl, 0.0, start_time, end_time, max_steps, 1, ctx->stream);
+    if (ctx->mixed) emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[0], ctx->ctl, emu::DT_INIT, ctx->stream);
+    else emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[0], ctx->ctl, emu::DT_INIT, ctx->stream);
+    return check_launch(ctx, "initial compute_dt");
+}
+
+int emu_evolve_steps(emu_context* ctx, int nsteps)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    int r;
+    for (int i = 0; i < nsteps; i++) {
+        if (!ctx->graph[ctx->cur] && (r = build_graph(ctx))) return r;
+        CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        ctx->cur_mesh = ctx->mixed ? 1 : 3;
+        if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
+            if ((r = resort(ctx))) return r;
+    }
+    return EMU_OK;
+}
+
+int emu_evolve_end(emu_context* ctx, emu_run_info* info)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    int r;
+    if ((r = sync_ctl(ctx))) return r;
+    const StepCtl& h = *ctx->ctl_host;
+    if (info) {
+        info->steps_done = h.step;
+        info->status = h.status;
+        info->bad_particle = h.bad == LLONG_MAX ? -1 : h.bad;
+        info->time = h.t;
+        info->dt_next = h.dt;
+    }
+    return status_of(ctx, nullptr);
+}
+
+int emu_evolve(emu_context* ctx, int nsteps, double start_time, double end_time, emu_run_info* info)
+{
+    int r;
+    if ((r = emu_evolve_begin(ctx, start_time, end_time, nsteps))) return r;
+    if ((r = emu_evolve_steps(ctx, nsteps))) return r;
+    return emu_evolve_end(ctx, info);
+}
+
+int emu_flush_l2(emu_context* ctx, void* buf, int64_t bytes)
+{
+    if (!ctx || !buf) return EMU_ERR_ARG;
+    emu::launch_flush(static_cast<double*>(buf), bytes / 8, ctx->stream);
+    return check_launch(ctx, "flush");
+}
+
+int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* nkernels)
+{
+    if (!ctx || !kernel_ms || !nkernels) return EMU_ERR_ARG;
+    if (!rk4_fused(ctx)) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: requires fused RK4");
+    const int nk = ctx->mixed ? 9 : 5;
+    if (max_kernels < nk) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
+    std::vector<cudaEvent_t> ev(2 * nk);
+    for (auto& e : ev) CU(cudaEventCreate(&e));
+    const DevState& S = ctx->S[ctx->cur];
+    cudaStream_t st = ctx->stream;
+    int k = 0;
+    auto rec = [&](int i) { return cudaEventRecord(ev[i], st); };
+    if (ctx->mixed) {
+        int a = 0;
+        for (int s = 1; s <= 4; s++) {
+            const int b = 1 - a;
+            rec(2 * k);
+            emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, st);
+            rec(2 * k + 1);
+            k++;
+            rec(2 * k);
+            emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->ctl, st);
+            rec(2 * k + 1);
+            k++;
+            a = b;
+        }
+        rec(2 * k);
+        emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[1], ctx->ctl, emu::DT_ADVANCE, st);
+        rec(2 * k + 1);
+        k++;
+    } else {
+        for (int s = 1; s <= 4; s++) {
+            rec(2 * k);
+            emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4],
+                                  ctx->mesh[(s + 1) % 4], mesh_elems(ctx), ctx->ctl, st);
+            rec(2 * k + 1);
+            k++;
+        }
+        rec(2 * k);
+        emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[3], ctx->ctl, emu::DT_ADVANCE, st);
+        rec(2 * k + 1);
+        k++;
+    }
+    int r = check_launch(ctx, "profile step");
+    if (r) return r;
+    ctx->cur_mesh = ctx->mixed ? 1 : 3;
+    CU(cudaStreamSynchronize(st));
+    for (int i = 0; i < k; i++) CU(cudaEventElapsedTime(&kernel_ms[i], ev[2 * i], ev[2 * i + 1]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    *nkernels = k;
+    if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
+        if ((r = resort(ctx))) return r;
+    return EMU_OK;
+}
+
+int emu_write_plotfile(emu_context* ctx, const char* dir, double time, int step, int write_particles)
+{
+    if (!ctx || !dir) return fail(ctx, EMU_ERR_ARG, "emu_write_plotfile: bad arguments");
+    const long long nc = ctx->P.ncells;
+    std::vector<double> mesh((size_t)nc * emu_ncomp(ctx->nf));
+    int r;
+    if ((r = emu_get_mesh(ctx, mesh.data()))) return r;
+    std::vector<double> parts;
+    int64_t n = 0;
+    if (write_particles) {
+        emu_num_particles(ctx, &n);
+        parts.resize((size_t)n * ctx->nreal);
+        if ((r = emu_get_particles(ctx, parts.data(), n))) return r;
+    }
+    std::string why;
+    if (!emu_host::write_plotfile(ctx->prm, dir, time, step, mesh.data(), write_particles ? parts.data() : nullptr,
+                                  n, why))
+        return fail(ctx, EMU_ERR_IO, "emu_write_plotfile: " + why);
+    return EMU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,341 @@
+// emu_device.cuh -- device-side building blocks of the Emu evolution path on
+// sm_100a: Hermitian component layout, shape factors, the interpolated
+// potential, the commutator right-hand side, renormalisation and the
+// warp-cooperative deposit.
+//
+// Reference semantics (paths relative to the Emu tree):
+//   shape factors        Source/ParticleInterpolator.H:34-131
+//   deposit              Source/Evolve.cpp:126-161, generate_code.py:150-169
+//   potentials           Source/Evolve.cpp:163-193, generate_code.py:239-357
+//   commutator RHS       Source/Evolve.cpp:195-210, generate_code.py:359-389
+//   Renormalize          Source/FlavoredNeutrinoContainer.cpp:89-113,
+//                        generate_code.py:391-445
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace emu {
+
+// Source/Constants.H:6-26
+constexpr double kC = 2.99792458e10;
+constexpr double kHbar = 1.05457266e-27;
+constexpr double kMp = 1.6726219e-24;
+constexpr double kEV = 1.60218e-12;
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// status bits shared with include/emu_b200.h
+enum : int { ST_TRACE = 1, ST_NEGDIAG = 2, ST_LENGTH = 4, ST_DT = 8 };
+
+// ---------------------------------------------------------------------------
+// Hermitian component layout: upper triangle, row-major, Re before Im
+// (Scripts/symbolic_hermitians/HermitianUtils.py:170-178).
+template <int NF>
+struct Herm {
+    static constexpr int NH = NF * NF;
+    // row i starts at sum_{r<i} (1 + 2(NF-1-r)) = i(2NF - i)
+    __host__ __device__ static constexpr int re(int i, int j)
+    {
+        return i * (2 * NF - i) + (j == i ? 0 : 2 * (j - i) - 1);
+    }
+    __host__ __device__ static constexpr int im(int i, int j) { return re(i, j) + 1; }
+    __host__ __device__ static constexpr bool is_diag(int e)
+    {
+        return NF == 2 ? (e == 0 || e == 3) : (e == 0 || e == 5 || e == 8);
+    }
+    __host__ __device__ static constexpr bool is_im(int e)
+    {
+        return NF == 2 ? (e == 2) : (e == 2 || e == 4 || e == 7);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Geometry and physics constants handed to every kernel by value.
+struct DevParams {
+    int nf;
+    int n[3];          // cells per dimension
+    int w[3];          // stencil width per dimension (order+1, order 0 for 1-cell dims)
+    int ord[3];        // shape order per dimension
+    long long ncells;
+    double L[3];       // domain length (periodic, [0,L))
+    double dxi[3];     // inverse cell size
+    double sqrt2GF_inv_vol;   // sqrt(2)*GF*inv_cell_volume (Evolve.cpp:167 + fill)
+    double matter;            // rho*Ye/Mp/inv_cell_volume (uniform background)
+    double M2[2][9];          // vacuum mass-squared matrix, nu and nubar (conjugated)
+    double c4;                // c^4
+    double inv_hbar;
+    double maxError;
+    double cell_volume;
+    double sqrt2GF;
+    double GF;
+    double rho, Ye;
+    double cfl_factor, flavor_cfl_factor, max_adaptive_speedup;
+    double dt_translation;
+    double vvac_max;
+    // mixed path: int64 fixed point scales per species and the factor that
+    // turns an integer mesh sum back into sqrt(2) GF n (erg)
+    double q_scale[2];        // contribution * q_scale -> integer
+    double q_unscale[2];      // integer * q_unscale -> number (same units as FP64 mesh)
+};
+
+// ---------------------------------------------------------------------------
+// ParticleInterpolator (Source/ParticleInterpolator.H:34-131).  The nearest
+// index uses C truncation (static_cast<int>), reproduced exactly.
+template <class R>
+__device__ __forceinline__ void shape(double delta, int order, int& first, R w[3])
+{
+    double dstar = (delta - 0.5 < 0.0) ? delta - 1.0 : delta;
+    int nearest = (int)dstar;
+    double fraction = delta - (double)(int)delta;
+    double offset = (delta <= 0.0) ? fraction + 0.5 : fraction - 0.5;
+    if (order >= 2) {
+        first = nearest - 1;
+        w[0] = (R)(0.5 * (0.5 - offset) * (0.5 - offset));
+        w[1] = (R)(0.75 - offset * offset);
+        w[2] = (R)(0.5 * (0.5 + offset) * (0.5 + offset));
+    } else if (order == 1) {
+        if (offset >= 0) {
+            first = nearest;
+            w[0] = (R)(1.0 - offset);
+            w[1] = (R)offset;
+        } else {
+            first = nearest - 1;
+            w[0] = (R)(-offset);
+            w[1] = (R)(1.0 + offset);
+        }
+        w[2] = (R)0;
+    } else {
+        first = nearest;
+        w[0] = (R)1;
+        w[1] = w[2] = (R)0;
+    }
+}
+
+__device__ __forceinline__ int wrapi(int a, int n)
+{
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// Stencil of one particle: first cell per dimension (wrapped) and weights.
+template <class R>
+struct Stencil {
+    int b[3];      // first cell, already wrapped into [0,n)
+    R wx[3], wy[3], wz[3];
+};
+
+template <class R>
+__device__ __forceinline__ void make_stencil(const DevParams& P, double x, double y, double z, Stencil<R>& s)
+{
+    int f;
+    shape<R>(x * P.dxi[0], P.ord[0], f, s.wx); s.b[0] = wrapi(f, P.n[0]);
+    shape<R>(y * P.dxi[1], P.ord[1], f, s.wy); s.b[1] = wrapi(f, P.n[1]);
+    shape<R>(z * P.dxi[2], P.ord[2], f, s.wz); s.b[2] = wrapi(f, P.n[2]);
+}
+
+__device__ __forceinline__ int stencil_key(const DevParams& P, const int b[3])
+{
+    return (b[2] * P.n[1] + b[1]) * P.n[0] + b[0];
+}
+
+__device__ __forceinline__ long long cell_of(const DevParams& P, int bx, int by, int bz, int ii, int jj, int kk)
+{
+    int i = bx + ii; if (i >= P.n[0]) i -= P.n[0];
+    int j = by + jj; if (j >= P.n[1]) j -= P.n[1];
+    int k = bz + kk; if (k >= P.n[2]) k -= P.n[2];
+    return ((long long)k * P.n[1] + j) * P.n[0] + i;
+}
+
+// ---------------------------------------------------------------------------
+// -i/hbar [H, F] in real components (generate_code.py:359-389), both given as
+// Hermitian component arrays.  Fully unrolled; the index algebra folds at
+// compile time.
+template <int NF, class R>
+__device__ __forceinline__ void commutator(const R* h, const R* f, R* out, R inv_hbar)
+{
+    using H = Herm<NF>;
+    R HR[NF][NF], HI[NF][NF], FR[NF][NF], FI[NF][NF];
+#pragma unroll
+    for (int i = 0; i < NF; i++)
+#pragma unroll
+        for (int j = i; j < NF; j++) {
+            HR[i][j] = h[H::re(i, j)];
+            FR[i][j] = f[H::re(i, j)];
+            if (j > i) {
+                HI[i][j] = h[H::im(i, j)];
+                FI[i][j] = f[H::im(i, j)];
+                HR[j][i] = HR[i][j]; HI[j][i] = -HI[i][j];
+                FR[j][i] = FR[i][j]; FI[j][i] = -FI[i][j];
+            } else {
+                HI[i][i] = (R)0;
+                FI[i][i] = (R)0;
+            }
+        }
+#pragma unroll
+    for (int i = 0; i < NF; i++)
+#pragma unroll
+        for (int j = i; j < NF; j++) {
+            R cr = (R)0, ci = (R)0;
+#pragma unroll
+            for (int k = 0; k < NF; k++) {
+                cr += HR[i][k] * FR[k][j] - HI[i][k] * FI[k][j];
+                ci += HR[i][k] * FI[k][j] + HI[i][k] * FR[k][j];
+                cr -= FR[i][k] * HR[k][j] - FI[i][k] * HI[k][j];
+                ci -= FR[i][k] * HI[k][j] + FI[i][k] * HR[k][j];
+            }
+            out[H::re(i, j)] = ci * inv_hbar;
+            if (j > i) out[H::im(i, j)] = -cr * inv_hbar;
+        }
+}
+
+// SU(n) flavour-vector length (HermitianUtils.py:102-123), summation in the
+// order of the generated expression: Im^2 then Re^2 per off-diagonal pair,
+// then the Cartan terms.
+template <int NF>
+__device__ __forceinline__ double su_length(const double* f)
+{
+    using H = Herm<NF>;
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NF; i++)
+#pragma unroll
+        for (int j = i + 1; j < NF; j++) {
+            double a = f[H::im(i, j)], b = f[H::re(i, j)];
+            s = __dadd_rn(s, __dmul_rn(a, a));
+            s = __dadd_rn(s, __dmul_rn(b, b));
+        }
+#pragma unroll
+    for (int l = 1; l < NF; l++) {
+        const double cl = (l == 1) ? 0.5 : 0.28867513459481287;   // sqrt(2/(l(l+1)))/2
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < l; i++) t = __dadd_rn(t, __dmul_rn(cl, f[H::re(i, i)]));
+        t = __dsub_rn(t, __dmul_rn(cl * l, f[H::re(l, l)]));
+        s = __dadd_rn(s, __dmul_rn(t, t));
+    }
+    return sqrt(s);
+}
+
+// Renormalize one species (generate_code.py:391-445).  Returns status bits
+// instead of aborting.
+template <int NF>
+__device__ __forceinline__ int renormalize(double* f, double L, double maxError)
+{
+    using H = Herm<NF>;
+    int st = 0;
+    double sumP = 0.0;
+#pragma unroll
+    for (int i = 0; i < NF; i++) sumP = __dadd_rn(sumP, f[H::re(i, i)]);
+    double error = sumP - 1.0;
+    if (fabs(error) > 100. * maxError) st |= ST_TRACE;
+    if (fabs(error) > maxError) {
+#pragma unroll
+        for (int i = 0; i < NF; i++) f[H::re(i, i)] = __dsub_rn(f[H::re(i, i)], __ddiv_rn(error, (double)NF));
+    }
+#pragma unroll
+    for (int i = 0; i < NF; i++) {
+        if (f[H::re(i, i)] < -100. * maxError) st |= ST_NEGDIAG;
+        if (f[H::re(i, i)] < -maxError) f[H::re(i, i)] = 0;
+    }
+    double length = su_length<NF>(f);
+    error = length - L;
+    if (fabs(error) > 100. * maxError) st |= ST_LENGTH;
+    if (fabs(error) > maxError) {
+        double r = __ddiv_rn(length, L);
+#pragma unroll
+        for (int e = 0; e < H::NH; e++) f[e] = __ddiv_rn(f[e], r);
+    }
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// Warp reduction of 32 values per lane: afterwards lane l holds the sum over
+// the warp of value index l (recursive halving, 31 shuffles per 32 values).
+template <class T>
+__device__ __forceinline__ T warp_transpose_sum(T (&v)[32])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const bool upper = (lane & off) != 0;
+#pragma unroll
+        for (int i = 0; i < off; i++) {
+            T send = upper ? v[i] : v[i + off];
+            T keep = upper ? v[i + off] : v[i];
+            T recv = __shfl_xor_sync(kFull, send, off);
+            v[i] = keep + recv;
+        }
+    }
+    return v[0];
+}
+
+__device__ __forceinline__ void atomic_add_mesh(double* p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_mesh(long long* p, long long v)
+{
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+}
+
+// Warp-cooperative deposit.  Every lane of the warp must call it (inactive
+// lanes pass key < 0).  Lanes sharing a stencil (same key) are reduced in
+// registers and one atomic per (cell, component) is issued; with many
+// distinct stencils in a warp each lane adds its own contributions.
+//   val(q, r) returns the contribution of component q (GIdx order minus 3)
+//   before the stencil weight r is applied; conv() turns weight*value into
+//   the accumulation type.
+template <int ND, int MAXG, class T, class W, class ValFn, class Conv>
+__device__ __forceinline__ void warp_deposit(const DevParams& P, T* mesh, int key, const Stencil<W>& st,
+                                             ValFn val, Conv conv)
+{
+    const int lane = threadIdx.x & 31;
+    constexpr int NR = (ND + 31) / 32;
+    const unsigned peers = __match_any_sync(kFull, key);
+    const bool leader = (__ffs(peers) - 1) == lane;
+    unsigned leaders = __ballot_sync(kFull, leader && key >= 0);
+    const int ng = __popc(leaders);
+    if (ng == 0) return;
+    if (ng <= MAXG) {
+        while (leaders) {
+            const int ld = __ffs(leaders) - 1;
+            leaders &= leaders - 1;
+            const int gkey = __shfl_sync(kFull, key, ld);
+            const bool mine = (key == gkey);
+            const int bx = gkey % P.n[0];
+            const int by = (gkey / P.n[0]) % P.n[1];
+            const int bz = gkey / (P.n[0] * P.n[1]);
+            for (int kk = 0; kk < P.w[2]; kk++)
+                for (int jj = 0; jj < P.w[1]; jj++)
+                    for (int ii = 0; ii < P.w[0]; ii++) {
+                        const W wgt = mine ? st.wx[ii] * st.wy[jj] * st.wz[kk] : (W)0;
+                        const long long cell = cell_of(P, bx, by, bz, ii, jj, kk);
+#pragma unroll
+                        for (int r = 0; r < NR; r++) {
+                            T v[32];
+#pragma unroll
+                            for (int i = 0; i < 32; i++) {
+                                const int q = r * 32 + i;
+                                v[i] = (mine && q < ND) ? conv(wgt, val(q), q) : (T)0;
+                            }
+                            T tot = warp_transpose_sum<T>(v);
+                            const int q = r * 32 + lane;
+                            if (q < ND && tot != (T)0) atomic_add_mesh(&mesh[cell * ND + q], tot);
+                        }
+                    }
+        }
+    } else {
+        if (key < 0) return;
+        for (int kk = 0; kk < P.w[2]; kk++)
+            for (int jj = 0; jj < P.w[1]; jj++)
+                for (int ii = 0; ii < P.w[0]; ii++) {
+                    const W wgt = st.wx[ii] * st.wy[jj] * st.wz[kk];
+                    const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
+#pragma unroll 4
+                    for (int q = 0; q < ND; q++) {
+                        T c = conv(wgt, val(q), q);
+                        if (c != (T)0) atomic_add_mesh(&mesh[cell * ND + q], c);
+                    }
+                }
+    }
+}
+
+}  // namespace emu

@@ -1,0 +1,32 @@
+// emu_host.h -- host-only helpers of the C ABI (no CUDA): physical constants,
+// parameter validation, the vacuum mass matrix, fixed-point scales, and the
+// AMReX plotfile / particle checkpoint writer.
+#pragma once
+
+#include <string>
+
+#include "emu_b200.h"
+
+namespace emu_host {
+
+// Source/Constants.H:6-26, evaluated in the same operation order
+double c2();
+double c4();
+double hbarc();
+double gf();
+
+bool validate(const emu_params& p, std::string& why);
+
+// flavour-basis mass-squared matrix in Hermitian component order for nu
+// (m2[0]) and nubar (m2[1], conjugated), generate_code.py:174-255
+void vacuum_m2(const emu_params& p, double m2[2][9]);
+
+// int64 fixed-point scales for the mixed deposit: contribution * scale is an
+// integer with |sum over any cell| < 2^62 (bound: total N per species)
+bool fixed_point_scales(const emu_params& p, const double* records, long long n, double scale[2],
+                        double unscale[2], std::string& why);
+
+bool write_plotfile(const emu_params& p, const char* dir, double time, int step, const double* mesh,
+                    const double* records, long long n, std::string& why);
+
+}  // namespace emu_host

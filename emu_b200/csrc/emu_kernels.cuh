@@ -1,0 +1,98 @@
+// emu_kernels.cuh -- device data layout and the host-side launchers of the
+// evolution kernels (implemented in emu_kernels.cu).
+//
+// HBM layout (structure of arrays, particles cell-sorted, stride = cap):
+//   pos[3], time, pup[4], Nn[2] (N, Nbar), Ll[2] (L, Lbar)        FP64
+//   vhat[3] = pup/pupt, vscale = c^4/(2 pupt)                       FP64
+//   f0[2*NF*NF]  state at the start of the step (nu then nubar)    FP64
+//   fs, acc      fused RK4: stage state and running RK sum         FP64
+//   kgen         unfused integrators: one RHS per stage            FP64
+//   k32, ksum32  mixed RK4: previous stage RHS and weighted sum    FP32
+//   vhat32[3], N32[2]  mixed copies of the static fields           FP32
+//   id           load index of each particle                       int64
+// Meshes are cell-major: mesh[cell*ND + q] with q in GIdx order minus 3
+// (ND = 8*NF*NF), FP64 (plain) or int64 fixed point (mixed).
+#pragma once
+
+#include "emu_device.cuh"
+
+namespace emu {
+
+struct DevState {
+    long long n = 0, cap = 0;
+    double* pos[3] = {};
+    double* time = nullptr;
+    double* pup[4] = {};
+    double* Nn[2] = {};
+    double* Ll[2] = {};
+    double* vhat[3] = {};
+    double* vscale = nullptr;
+    double* f0 = nullptr;
+    double* fs = nullptr;
+    double* acc = nullptr;
+    double* kgen = nullptr;        // [ns][2NH][cap]
+    float* k32 = nullptr;
+    float* ksum32 = nullptr;
+    float* vhat32[3] = {};
+    float* N32[2] = {};
+    long long* id = nullptr;
+};
+
+// Device-side step control: the timestep, time and error state live on the
+// device so that whole runs proceed without host round trips.
+struct StepCtl {
+    double dt;           // timestep of the step in progress
+    double t;            // integrator time at the start of the step in progress
+    double end_time;
+    long long bad;       // smallest load index that failed Renormalize (LLONG_MAX: none)
+    int status;          // OR of status bits
+    int done;            // 1: no more steps; stage kernels return immediately
+    int step;            // steps completed
+    int max_step;        // stop once this many steps are completed
+    int last;            // the step in progress is the final one (clipped to end_time)
+    unsigned int blocks_done;
+    unsigned long long vmax_bits[2];   // max V_adaptive, V_stupid (non-negative doubles as bits)
+};
+
+enum DtMode : int { DT_QUERY = 0, DT_INIT = 1, DT_ADVANCE = 2 };
+
+constexpr int kBlock = 256;
+
+// launchers (all asynchronous on the given stream)
+void launch_pack(int nf, const DevParams& P, const double* aos, const unsigned* perm, long long n, DevState S,
+                 cudaStream_t st);
+void launch_unpack(int nf, const DevState& S, double* aos, cudaStream_t st);
+void launch_unpack_rhs(int nf, const DevState& S, const double* K, double* aos, cudaStream_t st);
+void launch_cell_keys(const DevParams& P, const double* aos, int nreal, long long n, unsigned* keys,
+                      unsigned* idx, cudaStream_t st);
+void launch_deposit(int nf, const DevParams& P, const DevState& S, const double* f, double* mesh, cudaStream_t st);
+void launch_deposit_q(int nf, const DevParams& P, const DevState& S, const double* f, long long* mesh,
+                      cudaStream_t st);
+void launch_rhs(int nf, const DevParams& P, const DevState& S, const double* f, const double* mesh, double* K,
+                cudaStream_t st);
+void launch_stage_state(int nf, const DevState& S, const double* K, int nterms, const double* coef, double* out,
+                        cudaStream_t st);
+void launch_combine(int nf, const DevParams& P, const DevState& S, const double* K, int ns, const double* b,
+                    StepCtl* ctl, cudaStream_t st);
+void launch_rk4_stage(int nf, const DevParams& P, const DevState& S, int s, const double* mesh_in,
+                      double* mesh_out, double* mesh_zero, long long nzero, StepCtl* ctl, cudaStream_t st);
+void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
+                            long long* qmesh_out, StepCtl* ctl, cudaStream_t st);
+void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
+                           StepCtl* ctl, cudaStream_t st);
+void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st);
+void launch_dt_q(int nf, const DevParams& P, const long long* mesh, StepCtl* ctl, int mode, cudaStream_t st);
+void launch_renorm(int nf, const DevParams& P, const DevState& S, StepCtl* ctl, cudaStream_t st);
+void launch_mesh_out(int nf, const DevParams& P, const double* mesh, double* out, cudaStream_t st);
+void launch_mesh_out_q(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st);
+void launch_q_to_f64(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st);
+void launch_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status,
+                    cudaStream_t st);
+void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st);
+void launch_flush(double* buf, long long n, cudaStream_t st);
+// cell re-sort: keys of the current positions, then gather every array
+void launch_state_keys(const DevParams& P, const DevState& S, unsigned* keys, unsigned* idx, cudaStream_t st);
+void launch_gather_state(int nf, bool mixed, const DevState& src, const DevState& dst, const unsigned* perm,
+                         cudaStream_t st);
+
+}  // namespace emu

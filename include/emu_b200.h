@@ -1,0 +1,213 @@
+/*
+ * emu_b200.h -- C ABI of the B200 implementation of Emu's per-step particle
+ * evolution path (deposit_to_mesh -> interpolate_rhs_from_mesh -> Runge-Kutta
+ * stage update -> periodic wrap -> Renormalize -> compute_dt).
+ *
+ * Plain C types only: pointers, sizes, status codes.  Every entry point
+ * returns EMU_OK (0) or an OR of EMU_ERR_* bits and never aborts the process;
+ * emu_last_error() gives the message.  Reference functions are cited as
+ * file:line in the Emu source tree (AMReX-Astro/Emu).
+ *
+ * Particle records (host side) are FP64 rows of emu_nreal(nflavors) values:
+ *   pos_x, pos_y, pos_z, then the PIdx attributes
+ *   time,x,y,z,pupx,pupy,pupz,pupt,N,L,f..,Nbar,Lbar,f..bar
+ * (Source/FlavoredNeutrinoContainer.H:12-26 + generated H_fill), i.e. the
+ * real-component order of the reference's particle output
+ * (Scripts/visualization/amrex_plot_tools.py:12-90).
+ *
+ * Mesh output is emu_ncomp(nflavors) planes of ncell[0]*ncell[1]*ncell[2]
+ * FP64 values, i fastest, in GIdx order (Source/Evolve.H:11-27):
+ *   rho,T,Ye, N,Nbar,Fx,Fxbar,Fy,Fybar,Fz,Fzbar (each nflavors^2 reals).
+ */
+#ifndef EMU_B200_H_
+#define EMU_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMU_B200_ABI_VERSION 1
+
+/* status bits */
+#define EMU_OK           0
+#define EMU_ERR_TRACE    1     /* Renormalize: |trace-1| > 100*maxError   (generate_code.py:404-409) */
+#define EMU_ERR_NEGDIAG  2     /* Renormalize: diagonal < -100*maxError  (generate_code.py:418-423) */
+#define EMU_ERR_LENGTH   4     /* Renormalize: |length-L| > 100*maxError  (generate_code.py:433-438) */
+#define EMU_ERR_DT       8     /* compute_dt: no limiter active           (Evolve.cpp:119-121) */
+#define EMU_ERR_ARG      16    /* invalid argument */
+#define EMU_ERR_CUDA     32    /* CUDA runtime failure (no device, launch error, ...) */
+#define EMU_ERR_STATE    64    /* call out of order (e.g. no particles loaded) */
+#define EMU_ERR_IO       128   /* file I/O */
+#define EMU_ERR_PARSE    256   /* inputs file */
+#define EMU_ERR_NOMEM    512   /* allocation failed */
+#define EMU_ERR_LIMIT    1024  /* size beyond a documented limit */
+
+/* arithmetic of the path */
+#define EMU_PREC_FP64    0     /* FP64 throughout (the reference's PRECISION=DOUBLE) */
+#define EMU_PREC_MIXED   1     /* FP32 interpolation/potentials/commutator, int64
+                                  fixed-point deposit, FP64 rho accumulation,
+                                  renormalisation and vacuum+matter term */
+
+/*
+ * Run parameters.  Mirrors TestParams (Source/Parameters.H:11-132) in the
+ * reference's internal units: CGS, masses in grams, angles in radians (the
+ * inputs file's eV and degrees are converted by emu_parse_inputs exactly as
+ * Parameters.H:81-97 does).  The first five fields are the reference's
+ * compile-time choices (NUM_FLAVORS, SHAPE_FACTOR_ORDER, PRECISION) and the
+ * integrator keys (integration.type, integration.rk.type).
+ */
+typedef struct emu_params {
+    int nflavors;            /* 2 or 3 */
+    int shape_order;         /* 0, 1 or 2 */
+    int precision;           /* EMU_PREC_FP64 or EMU_PREC_MIXED */
+    int integration_type;    /* 0 forward Euler, 1 explicit Runge-Kutta */
+    int rk_type;             /* 2 trapezoid, 3 SSPRK3, 4 classical RK4 */
+
+    int ncell[3];
+    int nppc[3];
+    int nphi_equator;
+    double Lx, Ly, Lz;
+    int max_grid_size;
+    int nsteps;
+    double end_time;
+    int write_plot_every;
+    int write_plot_particles_every;
+    double rho_in, Ye_in, T_in;
+    int simulation_type;
+    double cfl_factor, flavor_cfl_factor, max_adaptive_speedup;
+    int do_restart;
+    char restart_dir[512];
+    double maxError;
+    double mass1, mass2, mass3;
+    double theta12, theta13, theta23;
+    double alpha1, alpha2, deltaCP;
+    int st3_wavelength_fraction_of_domain;
+    double st3_amplitude;
+    double st4_ndens, st4_theta, st4_phi, st4_fluxfac;
+    double st4_ndensbar, st4_thetabar, st4_phibar, st4_fluxfacbar;
+    double st4_amplitude;
+    double st5_nnue, st5_nnua, st5_nnux;
+    double st5_fxnue, st5_fxnua, st5_fxnux;
+    double st5_fynue, st5_fynua, st5_fynux;
+    double st5_fznue, st5_fznua, st5_fznux;
+    double st5_amplitude;
+
+    /* extensions of this implementation */
+    int direction_generator; /* 0: uniform_sphere_xyz ring generator (Init.cpp:9-37),
+                                1: Fibonacci sphere with ndirections points */
+    int ndirections;
+    uint64_t seed;           /* counter-based RNG seed for sim types 4 and 5
+                                (the reference seeds from the clock, main.cpp:240) */
+    int resort_interval;     /* steps between on-device cell re-sorts (0 = never) */
+    int fused;               /* 1: fused one-kernel-per-stage RK4 (default), 0: unfused stages */
+} emu_params;
+
+/* summary of a device-resident run (emu_evolve) */
+typedef struct emu_run_info {
+    int steps_done;          /* steps completed by this call */
+    int status;              /* OR of EMU_ERR_* raised on the device */
+    int64_t bad_particle;    /* load index of the first particle that failed Renormalize, or -1 */
+    double time;             /* integrator time after the last completed step */
+    double dt_next;          /* timestep the next step would take (compute_dt on the last stage mesh) */
+} emu_run_info;
+
+typedef struct emu_context emu_context;
+
+/* ---- sizes ---- */
+int emu_nattribs(int nflavors);        /* PIdx::nattribs: 20 or 30 */
+int emu_nreal(int nflavors);           /* 3 + nattribs */
+int emu_ncomp(int nflavors);           /* GIdx::ncomp: 35 or 75 */
+int emu_abi_version(void);
+
+/* ---- configuration (host only, no GPU needed) ---- */
+/* Defaults for every field (the values of Emu's sample inputs where one exists). */
+void emu_params_default(emu_params* p);
+/* Reads an inputs file plus "key=value" overrides with ParmParse syntax and
+ * unit conversion (replaces TestParams::Initialize, Parameters.H:52-131).
+ * Every key the reference requires is required here too. */
+int emu_parse_inputs(const char* path, int n_overrides, const char* const* overrides,
+                     emu_params* out, char* errbuf, size_t errlen);
+/* Initial particles on the host (replaces FlavoredNeutrinoContainer::InitParticles,
+ * FlavoredNeutrinoContainerInit.cpp:136-661).  With out == NULL only *n_out is set. */
+int emu_init_particles(const emu_params* p, double* out, int64_t capacity, int64_t* n_out);
+/* Vvac_max of a particle set (FlavoredNeutrinoContainerInit.cpp:657-660). */
+int emu_vvac_max(const emu_params* p, const double* records, int64_t n, double* out);
+
+/* ---- context (needs a CUDA device) ---- */
+/* Creates the device context; the caller owns it. */
+int emu_create(const emu_params* p, emu_context** out);
+void emu_destroy(emu_context* ctx);
+/* Launch all work of this context on a caller-provided cudaStream_t (NULL =
+ * the context's own stream). */
+int emu_set_stream(emu_context* ctx, void* cuda_stream);
+int emu_synchronize(emu_context* ctx);
+
+/* Upload particle records (host memory).  Replaces InitParticles/Restart as the
+ * source of the container; particles are cell-sorted on the device. */
+int emu_load_particles(emu_context* ctx, const double* records, int64_t n);
+/* Download particle records in load order. */
+int emu_get_particles(emu_context* ctx, double* records, int64_t n);
+int emu_num_particles(const emu_context* ctx, int64_t* n);
+
+/* deposit_to_mesh (Evolve.H:31 / Evolve.cpp:126-161) of the current particles */
+int emu_deposit(emu_context* ctx);
+/* The current mesh (rho,T,Ye and the last deposit), GIdx planes. */
+int emu_get_mesh(emu_context* ctx, double* out);
+/* interpolate_rhs_from_mesh (Evolve.H:33 / Evolve.cpp:163-211): the time
+ * derivative of every attribute of every particle, from the current mesh,
+ * written as particle records in load order (positions copied through). */
+int emu_interpolate_rhs(emu_context* ctx, double* rhs_records);
+/* FlavoredNeutrinoContainer::Renormalize (FlavoredNeutrinoContainer.H:92). */
+int emu_renormalize(emu_context* ctx, int64_t* bad_particle);
+/* compute_dt (Evolve.H:29 / Evolve.cpp:57-124) on the current mesh. */
+int emu_compute_dt(emu_context* ctx, double* dt);
+/* One integrator step of length dt (TimeIntegrator::advance with
+ * ApplyFlavoredNeutrinoRHS, FlavoredNeutrinoContainer.H:33-47) followed by the
+ * post-timestep hook (SyncLocation, periodic Redistribute, Renormalize,
+ * main.cpp:155-173).  Afterwards the current mesh is the last stage deposit. */
+int emu_step(emu_context* ctx, double dt, int64_t* bad_particle);
+/* The evolve_flavor loop (main.cpp:118,206,213): deposit, compute_dt, then up
+ * to nsteps steps (stopping at end_time, dt clipped to land on it), with dt
+ * recomputed on the device from each step's last stage mesh.  Runs without
+ * host synchronisation between steps.  start_time is the integrator time of
+ * the loaded particles. */
+int emu_evolve(emu_context* ctx, int nsteps, double start_time, double end_time, emu_run_info* info);
+/* emu_evolve in three parts, for callers that pipeline work on the stream:
+ * begin = deposit + initial compute_dt on the device; steps = enqueue that
+ * many steps (each a CUDA graph launch, no host synchronisation); end =
+ * synchronise and report.  Steps past max_steps or end_time do no work. */
+int emu_evolve_begin(emu_context* ctx, double start_time, double end_time, int max_steps);
+int emu_evolve_steps(emu_context* ctx, int nsteps);
+int emu_evolve_end(emu_context* ctx, emu_run_info* info);
+/* Overwrite a device buffer (bytes, multiple of 8) on the context's stream;
+ * benchmarks use it to evict the L2 cache between timed steps. */
+int emu_flush_l2(emu_context* ctx, void* device_buffer, int64_t bytes);
+/* One device-resident step (as emu_evolve_steps(ctx, 1)) launched kernel by
+ * kernel with a CUDA event pair around each launch on the context stream.
+ * kernel_ms[i] receives the duration of kernel i in launch order (the RK
+ * stages, then the compute_dt reduction); *nkernels their count.  Call after
+ * emu_evolve_begin. */
+int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* nkernels);
+
+/* Plotfile (IO.cpp:11-38): mesh plotfile pltNNNNN plus, when
+ * write_particles != 0, the particle checkpoint pltNNNNN/neutrinos. */
+int emu_write_plotfile(emu_context* ctx, const char* dir, double time, int step, int write_particles);
+/* The same plotfile from host arrays (mesh as emu_get_mesh returns it,
+ * records may be NULL): host only, no GPU needed. */
+int emu_write_plotfile_host(const emu_params* p, const char* dir, double time, int step, const double* mesh,
+                            const double* records, int64_t n);
+/* Particle checkpoint reader (RecoverParticles, IO.cpp:40-63): host only. */
+int emu_read_particles(const char* plotfile_dir, int nflavors, double* out, int64_t capacity,
+                       int64_t* n_out, double* time, int* step);
+
+/* Message of the last failure on this context (or of the last host-only call
+ * when ctx is NULL). */
+int emu_last_error(const emu_context* ctx, char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMU_B200_H_ */
