@@ -39,16 +39,19 @@ from emu_b200 import workloads as W  # noqa: E402
 METRIC = "particle RK4 steps/s on 1 B200: mixed vs FP64 at stated err; % of HBM peak"
 
 
-def workload(name, precision):
+def workload(name, precision, cells=None):
+    """cells overrides the cell count (z cells for c2/c3, cells per side for
+    c5) to run a smaller case of the same workload (profiling)."""
     if name == "c2":
-        p = W.c2_fast_flavor_1d()
-        desc = "C2 fast-flavor 1D: 2 flavors, 1x1x128 cells over 64 cm, 80 Fibonacci directions/cell"
+        p = W.c2_fast_flavor_1d(ncell_z=cells or 128)
+        desc = "C2 fast-flavor 1D: 2 flavors, 1x1x%d cells over %g cm, 80 Fibonacci directions/cell" % (
+            p.ncell[2], p.Lz)
     elif name == "c3":
-        p = W.c3_three_flavor_1d()
-        desc = "C3 3-flavor 1D: 1x1x1024 cells, 378 ring directions/cell"
+        p = W.c3_three_flavor_1d(ncell_z=cells or 1024)
+        desc = "C3 3-flavor 1D: 1x1x%d cells, 378 ring directions/cell" % p.ncell[2]
     elif name == "c5":
-        p = W.c5_3d()
-        desc = "C5 3-flavor 3D: 64^3 cells x 96 Fibonacci directions"
+        p = W.c5_3d(n=cells or 64)
+        desc = "C5 3-flavor 3D: %d^3 cells x 96 Fibonacci directions" % p.ncell[0]
     else:
         raise SystemExit("unknown workload " + name)
     if precision:
@@ -161,7 +164,7 @@ def run_reference(args):
     ws, rank, local = dist_setup(args)
     if rank != 0:
         return
-    p, desc = workload(args.workload, args.precision)
+    p, desc = workload(args.workload, args.precision, args.cells)
     recs = api.init_particles(p)
     nthreads = os.cpu_count() or 1
     from oracle.oracle import Oracle, RefHarness, have_ref
@@ -206,7 +209,7 @@ def run_emu(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    p, desc = workload(args.workload, args.precision)
+    p, desc = workload(args.workload, args.precision, args.cells)
     mixed = p.precision == api.PREC_MIXED
     nf = p.nflavors
     recs = api.init_particles(p)
@@ -344,6 +347,7 @@ def main():
     ap.add_argument("--impl", default="emu", choices=["emu", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"])
+    ap.add_argument("--cells", type=int, default=None, help="smaller case of the workload (cells per side)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=15.0)

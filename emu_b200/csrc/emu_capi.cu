@@ -300,8 +300,7 @@ int enqueue_rk4_fp64(emu_context* ctx, cudaStream_t st, bool with_dt)
     const DevState& S = ctx->S[ctx->cur];
     for (int s = 1; s <= 4; s++)
         emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4], ctx->mesh[(s + 1) % 4],
-                              mesh_elems(ctx), ctx->ctl, st);
-    if (with_dt) emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[3], ctx->ctl, emu::DT_ADVANCE, st);
+                              mesh_elems(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
     return check_launch(ctx, "rk4 stage");
 }
 
@@ -313,11 +312,12 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt)
     for (int s = 1; s <= 4; s++) {
         const int b = 1 - a;
         emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, st);
-        emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->ctl, st);
+        // M_4 sits in q[1] (read by stage 4's compute_dt) until the next
+        // step's first finalize zeroes it
+        emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->qmesh[1], ctx->ctl,
+                                    (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
         a = b;
     }
-    // M_4 sits in q[1] until the next step's first finalize zeroes it
-    if (with_dt) emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[1], ctx->ctl, emu::DT_ADVANCE, st);
     return check_launch(ctx, "rk4 mixed stage");
 }
 
@@ -773,7 +773,7 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
 {
     if (!ctx || !kernel_ms || !nkernels) return EMU_ERR_ARG;
     if (!rk4_fused(ctx)) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: requires fused RK4");
-    const int nk = ctx->mixed ? 9 : 5;
+    const int nk = ctx->mixed ? 8 : 4;
     if (max_kernels < nk) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
     std::vector<cudaEvent_t> ev(2 * nk);
     for (auto& e : ev) CU(cudaEventCreate(&e));
@@ -790,27 +790,21 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
             rec(2 * k + 1);
             k++;
             rec(2 * k);
-            emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->ctl, st);
+            emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->qmesh[1], ctx->ctl,
+                                        s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
             a = b;
         }
-        rec(2 * k);
-        emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[1], ctx->ctl, emu::DT_ADVANCE, st);
-        rec(2 * k + 1);
-        k++;
     } else {
         for (int s = 1; s <= 4; s++) {
             rec(2 * k);
             emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4],
-                                  ctx->mesh[(s + 1) % 4], mesh_elems(ctx), ctx->ctl, st);
+                                  ctx->mesh[(s + 1) % 4], mesh_elems(ctx), ctx->ctl,
+                                  s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
         }
-        rec(2 * k);
-        emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[3], ctx->ctl, emu::DT_ADVANCE, st);
-        rec(2 * k + 1);
-        k++;
     }
     int r = check_launch(ctx, "profile step");
     if (r) return r;

@@ -250,21 +250,44 @@ __device__ __forceinline__ int renormalize(double* f, double L, double maxError)
 }
 
 // ---------------------------------------------------------------------------
-// Warp reduction of 32 values per lane: afterwards lane l holds the sum over
-// the warp of value index l (recursive halving, 31 shuffles per 32 values).
-template <class T>
-__device__ __forceinline__ T warp_transpose_sum(T (&v)[32])
+// Stencil widths as template parameters: WX/WY/WZ in {1,2,3} are fixed
+// widths, 0 means "runtime width up to 3".  Loops over the stencil are fully
+// unrolled so that the weights and per-cell values stay in registers.
+template <int WX, int WY, int WZ>
+struct SW {
+    static constexpr int MX = WX ? WX : 3, MY = WY ? WY : 3, MZ = WZ ? WZ : 3;
+    __device__ __forceinline__ static bool on(const DevParams& P, int ii, int jj, int kk)
+    {
+        return (WX || ii < P.w[0]) && (WY || jj < P.w[1]) && (WZ || kk < P.w[2]);
+    }
+};
+
+// Warp reduction of 32 values per lane, produced on the fly by gen(i):
+// afterwards lane l holds the sum over the warp of value index l (recursive
+// halving, 31 shuffles per 32 values, at most 16 values live).
+template <class T, class Gen>
+__device__ __forceinline__ T warp_transpose_sum(Gen gen)
 {
     const int lane = threadIdx.x & 31;
+    T v[16];
+    {
+        const bool upper = (lane & 16) != 0;
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) {
+        for (int i = 0; i < 16; i++) {
+            const T a = gen(i), b = gen(i + 16);
+            const T send = upper ? a : b;
+            const T keep = upper ? b : a;
+            v[i] = keep + __shfl_xor_sync(kFull, send, 16);
+        }
+    }
+#pragma unroll
+    for (int off = 8; off >= 1; off >>= 1) {
         const bool upper = (lane & off) != 0;
 #pragma unroll
         for (int i = 0; i < off; i++) {
-            T send = upper ? v[i] : v[i + off];
-            T keep = upper ? v[i + off] : v[i];
-            T recv = __shfl_xor_sync(kFull, send, off);
-            v[i] = keep + recv;
+            const T send = upper ? v[i] : v[i + off];
+            const T keep = upper ? v[i + off] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, off);
         }
     }
     return v[0];
@@ -283,7 +306,122 @@ __device__ __forceinline__ void atomic_add_mesh(long long* p, long long v)
 //   val(q, r) returns the contribution of component q (GIdx order minus 3)
 //   before the stencil weight r is applied; conv() turns weight*value into
 //   the accumulation type.
-template <int ND, int MAXG, class T, class W, class ValFn, class Conv>
+// ---------------------------------------------------------------------------
+// Tile deposit.  The CTA's particles (consecutive in cell-sorted order) have
+// written one record each to shared memory:
+//   skey[i]             stencil key (first cell), -1 for no particle
+//   srec[i*RW + ...]    fN[2NF^2] = f*N per species, v[3], wx[3], wy[3], wz[3]
+// Threads then own deposit components q (GIdx order minus 3); each
+// accumulates w*f*N*v over a run of particles with the same key in
+// registers (27 accumulators in 3D, 3 in 1D) and adds the run total to the
+// mesh with one atomic per (cell, component) when the key changes.  With
+// ND = 32 (2 flavors) the CTA runs kBlock/32 independent particle streams.
+// Record layout (R = float or double): w[SP] stencil-weight products in
+// stencil order (kk, jj, ii), then fN[2NF^2], then v[3]; SP and the record
+// width RW are padded to 16 bytes so the weights load as 16-byte vectors.
+template <int NF, class SWt, class R>
+struct TileRec {
+    static constexpr int NS = 2 * NF * NF;
+    static constexpr int S = SWt::MX * SWt::MY * SWt::MZ;
+    static constexpr int VEC = 16 / (int)sizeof(R);
+    static constexpr int SP = (S + VEC - 1) / VEC * VEC;
+    static constexpr int RW = (SP + NS + 3 + VEC - 1) / VEC * VEC;
+};
+
+template <class R, int SP>
+__device__ __forceinline__ void load_weights(const R* r, R (&w)[SP])
+{
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll
+        for (int k = 0; k < SP; k += 4) {
+            const float4 v = *reinterpret_cast<const float4*>(r + k);
+            w[k] = v.x; w[k + 1] = v.y; w[k + 2] = v.z; w[k + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < SP; k += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(r + k);
+            w[k] = v.x; w[k + 1] = v.y;
+        }
+    }
+}
+
+template <int NF, int BLOCK, class SWt, class R, class T, class Conv>
+__device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const R* srec, int ntile,
+                                             Conv conv)
+{
+    using TR = TileRec<NF, SWt, R>;
+    constexpr int NH = NF * NF, NS = 2 * NH, ND = 8 * NH, RW = TR::RW, SP = TR::SP;
+    constexpr int NDP = (ND + 31) / 32 * 32;
+    constexpr int NSTREAM = BLOCK / NDP > 0 ? BLOCK / NDP : 1;
+    constexpr int SX = SWt::MX, SY = SWt::MY, SZ = SWt::MZ;
+    const int q = threadIdx.x % NDP;
+    const int stream = threadIdx.x / NDP;
+    if (stream >= NSTREAM || q >= ND) return;   // no block-wide barrier follows inside
+    const int dir = q / (2 * NH), sp = (q / NH) & 1, e = q % NH;
+    R acc[SZ * SY * SX];
+    auto flush = [&](int key) {
+        const int bx = key % P.n[0];
+        const int by = (key / P.n[0]) % P.n[1];
+        const int bz = key / (P.n[0] * P.n[1]);
+#pragma unroll
+        for (int kk = 0; kk < SZ; kk++)
+#pragma unroll
+            for (int jj = 0; jj < SY; jj++)
+#pragma unroll
+                for (int ii = 0; ii < SX; ii++) {
+                    if (!SWt::on(P, ii, jj, kk)) continue;
+                    const T v = conv(acc[(kk * SY + jj) * SX + ii], sp);
+                    if (v != (T)0) atomic_add_mesh(&mesh[cell_of(P, bx, by, bz, ii, jj, kk) * ND + q], v);
+                }
+    };
+    int cur = -1;
+    for (int i = stream; i < ntile; i += NSTREAM) {
+        const int key = skey[i];
+        if (key != cur) {
+            if (cur >= 0) flush(cur);
+#pragma unroll
+            for (int k = 0; k < SZ * SY * SX; k++) acc[k] = (R)0;
+            cur = key;
+        }
+        if (key < 0) continue;
+        const R* r = srec + i * RW;
+        const R b = r[SP + sp * NH + e];
+        const R qv = dir == 0 ? b : b * r[SP + NS + dir - 1];
+        R w[SP];
+        load_weights<R, SP>(r, w);
+#pragma unroll
+        for (int k = 0; k < SZ * SY * SX; k++) acc[k] += w[k] * qv;
+    }
+    if (cur >= 0) flush(cur);
+}
+
+// write one particle's deposit record (phase A of the tile deposit)
+template <int NF, class SWt, class R>
+__device__ __forceinline__ void tile_record(R* srec, int* skey, int i, int key, const R* fN, R vx, R vy, R vz,
+                                            const Stencil<R>& st)
+{
+    using TR = TileRec<NF, SWt, R>;
+    constexpr int NS = TR::NS, RW = TR::RW, SP = TR::SP;
+    skey[i] = key;
+    R* r = srec + i * RW;
+#pragma unroll
+    for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+        for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+            for (int ii = 0; ii < SWt::MX; ii++)
+                r[(kk * SWt::MY + jj) * SWt::MX + ii] = (st.wx[ii] * st.wy[jj]) * st.wz[kk];
+#pragma unroll
+    for (int k = TR::S; k < SP; k++) r[k] = (R)0;
+#pragma unroll
+    for (int c = 0; c < NS; c++) r[SP + c] = fN[c];
+    r[SP + NS + 0] = vx;
+    r[SP + NS + 1] = vy;
+    r[SP + NS + 2] = vz;
+}
+
+template <int ND, int MAXG, class SWt, class T, class W, class ValFn, class Conv>
 __device__ __forceinline__ void warp_deposit(const DevParams& P, T* mesh, int key, const Stencil<W>& st,
                                              ValFn val, Conv conv)
 {
@@ -303,20 +441,21 @@ __device__ __forceinline__ void warp_deposit(const DevParams& P, T* mesh, int ke
             const int bx = gkey % P.n[0];
             const int by = (gkey / P.n[0]) % P.n[1];
             const int bz = gkey / (P.n[0] * P.n[1]);
-            for (int kk = 0; kk < P.w[2]; kk++)
-                for (int jj = 0; jj < P.w[1]; jj++)
-                    for (int ii = 0; ii < P.w[0]; ii++) {
+#pragma unroll
+            for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+                for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+                    for (int ii = 0; ii < SWt::MX; ii++) {
+                        if (!SWt::on(P, ii, jj, kk)) continue;
                         const W wgt = mine ? st.wx[ii] * st.wy[jj] * st.wz[kk] : (W)0;
                         const long long cell = cell_of(P, bx, by, bz, ii, jj, kk);
 #pragma unroll
                         for (int r = 0; r < NR; r++) {
-                            T v[32];
-#pragma unroll
-                            for (int i = 0; i < 32; i++) {
+                            const T tot = warp_transpose_sum<T>([&](int i) -> T {
                                 const int q = r * 32 + i;
-                                v[i] = (mine && q < ND) ? conv(wgt, val(q), q) : (T)0;
-                            }
-                            T tot = warp_transpose_sum<T>(v);
+                                return (mine && q < ND) ? conv(wgt, val(q), q) : (T)0;
+                            });
                             const int q = r * 32 + lane;
                             if (q < ND && tot != (T)0) atomic_add_mesh(&mesh[cell * ND + q], tot);
                         }
@@ -324,14 +463,18 @@ __device__ __forceinline__ void warp_deposit(const DevParams& P, T* mesh, int ke
         }
     } else {
         if (key < 0) return;
-        for (int kk = 0; kk < P.w[2]; kk++)
-            for (int jj = 0; jj < P.w[1]; jj++)
-                for (int ii = 0; ii < P.w[0]; ii++) {
+#pragma unroll
+        for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+            for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+                for (int ii = 0; ii < SWt::MX; ii++) {
+                    if (!SWt::on(P, ii, jj, kk)) continue;
                     const W wgt = st.wx[ii] * st.wy[jj] * st.wz[kk];
                     const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
-#pragma unroll 4
+#pragma unroll
                     for (int q = 0; q < ND; q++) {
-                        T c = conv(wgt, val(q), q);
+                        const T c = conv(wgt, val(q), q);
                         if (c != (T)0) atomic_add_mesh(&mesh[cell * ND + q], c);
                     }
                 }

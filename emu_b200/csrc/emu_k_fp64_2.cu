@@ -1,0 +1,10 @@
+// emu_k_fp64_2.cu -- FP64 stage / deposit / RHS kernels for 2 flavors.
+#include "emu_kernels_impl.cuh"
+
+namespace emu {
+template void launch_rk4_stage_t<2>(const DevParams&, const DevState&, int, const double*, double*, double*,
+                                    long long, StepCtl*, int, cudaStream_t);
+template void launch_deposit_t<2>(const DevParams&, const DevState&, const double*, double*, cudaStream_t);
+template void launch_rhs_t<2>(const DevParams&, const DevState&, const double*, const double*, double*,
+                              cudaStream_t);
+}  // namespace emu

@@ -1,0 +1,177 @@
+// emu_k_misc.cu -- launchers of the small kernels and the flavor-count
+// dispatch of the large ones (whose instantiations live in
+// emu_k_fp64_<nf>.cu and emu_k_mixed_<nf>.cu so that they compile in
+// parallel).
+#include "emu_kernels_impl.cuh"
+
+namespace emu {
+
+#define EMU_EXTERN(NF)                                                                                          \
+    extern template void launch_rk4_stage_t<NF>(const DevParams&, const DevState&, int, const double*, double*,  \
+                                                double*, long long, StepCtl*, int, cudaStream_t);                \
+    extern template void launch_deposit_t<NF>(const DevParams&, const DevState&, const double*, double*,         \
+                                              cudaStream_t);                                                     \
+    extern template void launch_rhs_t<NF>(const DevParams&, const DevState&, const double*, const double*,       \
+                                          double*, cudaStream_t);                                                \
+    extern template void launch_rk4_stage_mixed_t<NF>(const DevParams&, const DevState&, int, const float*,      \
+                                                      long long*, const long long*, StepCtl*, int, cudaStream_t); \
+    extern template void launch_deposit_q_t<NF>(const DevParams&, const DevState&, const double*, long long*,    \
+                                                cudaStream_t);
+EMU_EXTERN(2)
+EMU_EXTERN(3)
+
+#define EMU_NF_DISPATCH(nf, KERNEL_CALL) \
+    do {                                 \
+        if ((nf) == 2) {                 \
+            constexpr int NFv = 2;       \
+            KERNEL_CALL;                 \
+        } else {                         \
+            constexpr int NFv = 3;       \
+            KERNEL_CALL;                 \
+        }                                \
+    } while (0)
+
+
+void launch_pack(int nf, const DevParams& P, const double* aos, const unsigned* perm, long long n, DevState S,
+                 cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_pack<NFv><<<grid_for(n), kBlock, 0, st>>>(P, aos, perm, n, S)));
+}
+
+void launch_unpack(int nf, const DevState& S, double* aos, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_unpack<NFv><<<grid_for(S.n), kBlock, 0, st>>>(S, aos)));
+}
+
+void launch_unpack_rhs(int nf, const DevState& S, const double* K, double* aos, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_unpack_rhs<NFv><<<grid_for(S.n), kBlock, 0, st>>>(S, K, aos)));
+}
+
+void launch_cell_keys(const DevParams& P, const double* aos, int nreal, long long n, unsigned* keys, unsigned* idx,
+                      cudaStream_t st)
+{
+    k_cell_keys_aos<<<grid_for(n), kBlock, 0, st>>>(P, aos, nreal, n, keys, idx);
+}
+
+void launch_state_keys(const DevParams& P, const DevState& S, unsigned* keys, unsigned* idx, cudaStream_t st)
+{
+    k_cell_keys_soa<<<grid_for(S.n), kBlock, 0, st>>>(P, S, keys, idx);
+}
+
+void launch_gather_state(int nf, bool mixed, const DevState& src, const DevState& dst, const unsigned* perm,
+                         cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_gather_state<NFv><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, mixed ? 1 : 0)));
+}
+
+void launch_deposit(int nf, const DevParams& P, const DevState& S, const double* f, double* mesh, cudaStream_t st)
+{
+    if (nf == 2) launch_deposit_t<2>(P, S, f, mesh, st); else launch_deposit_t<3>(P, S, f, mesh, st);
+}
+
+void launch_deposit_q(int nf, const DevParams& P, const DevState& S, const double* f, long long* mesh,
+                      cudaStream_t st)
+{
+    if (nf == 2) launch_deposit_q_t<2>(P, S, f, mesh, st); else launch_deposit_q_t<3>(P, S, f, mesh, st);
+}
+
+void launch_rhs(int nf, const DevParams& P, const DevState& S, const double* f, const double* mesh, double* K,
+                cudaStream_t st)
+{
+    if (nf == 2) launch_rhs_t<2>(P, S, f, mesh, K, st); else launch_rhs_t<3>(P, S, f, mesh, K, st);
+}
+
+void launch_stage_state(int nf, const DevState& S, const double* K, int nterms, const double* coef, double* out,
+                        cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_stage_state<NFv><<<grid_for(S.n), kBlock, 0, st>>>(
+                            S, K, nterms, coef[0], nterms > 1 ? coef[1] : 0.0, nterms > 2 ? coef[2] : 0.0, out)));
+}
+
+void launch_combine(int nf, const DevParams& P, const DevState& S, const double* K, int ns, const double* b,
+                    StepCtl* ctl, cudaStream_t st)
+{
+    double w[4] = {0, 0, 0, 0};
+    for (int i = 0; i < ns && i < 4; i++) w[i] = b[i];
+    EMU_NF_DISPATCH(nf, (k_combine<NFv><<<grid_for(S.n), kBlock, 0, st>>>(P, S, K, ns, w[0], w[1], w[2], w[3], ctl)));
+}
+
+void launch_rk4_stage(int nf, const DevParams& P, const DevState& S, int s, const double* mesh_in, double* mesh_out,
+                      double* mesh_zero, long long nzero, StepCtl* ctl, int dt_mode, cudaStream_t st)
+{
+    if (nf == 2) launch_rk4_stage_t<2>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt_mode, st);
+    else launch_rk4_stage_t<3>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt_mode, st);
+}
+
+void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
+                            long long* qmesh_out, const long long* qmesh_dt, StepCtl* ctl, int dt_mode,
+                            cudaStream_t st)
+{
+    if (nf == 2) launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, ctl, dt_mode, st);
+    else launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, ctl, dt_mode, st);
+}
+
+static unsigned reduce_grid(long long ncells)
+{
+    long long g = (ncells + kBlock - 1) / kBlock;
+    if (g > 1184) g = 1184;
+    if (g < 1) g = 1;
+    return (unsigned)g;
+}
+
+void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
+                           StepCtl* ctl, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_finalize_mixed<NFv><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, qread, qzero, gmesh,
+                                                                                        ctl)));
+}
+
+void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_dt<NFv, double><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode)));
+}
+
+void launch_dt_q(int nf, const DevParams& P, const long long* mesh, StepCtl* ctl, int mode, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_dt<NFv, long long><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode)));
+}
+
+void launch_renorm(int nf, const DevParams& P, const DevState& S, StepCtl* ctl, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_renorm<NFv><<<grid_for(S.n), kBlock, 0, st>>>(P, S, ctl)));
+}
+
+void launch_mesh_out(int nf, const DevParams& P, const double* mesh, double* out, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_mesh_out<NFv><<<grid_for(P.ncells * 8 * NFv * NFv), kBlock, 0, st>>>(P, mesh, out)));
+}
+
+void launch_mesh_out_q(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_mesh_out_q<NFv><<<grid_for(P.ncells * 8 * NFv * NFv), kBlock, 0, st>>>(P, mesh, out)));
+}
+
+void launch_q_to_f64(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_q_to_f64<NFv><<<grid_for(P.ncells * 8 * NFv * NFv), kBlock, 0, st>>>(P, mesh, out)));
+}
+
+void launch_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status,
+                    cudaStream_t st)
+{
+    k_ctl_set<<<1, 1, 0, st>>>(ctl, dt, t, end_time, max_step, reset_status);
+}
+
+void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st)
+{
+    (void)nf;
+    k_mixed_shadow<<<grid_for(S.n), kBlock, 0, st>>>(S);
+}
+
+void launch_flush(double* buf, long long n, cudaStream_t st)
+{
+    k_flush<<<148 * 8, 256, 0, st>>>(buf, n);
+}
+
+}  // namespace emu

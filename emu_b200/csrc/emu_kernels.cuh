@@ -56,7 +56,7 @@ struct StepCtl {
 
 enum DtMode : int { DT_QUERY = 0, DT_INIT = 1, DT_ADVANCE = 2 };
 
-constexpr int kBlock = 256;
+constexpr int kBlock = 128;
 
 // launchers (all asynchronous on the given stream)
 void launch_pack(int nf, const DevParams& P, const double* aos, const unsigned* perm, long long n, DevState S,
@@ -74,10 +74,14 @@ void launch_stage_state(int nf, const DevState& S, const double* K, int nterms, 
                         cudaStream_t st);
 void launch_combine(int nf, const DevParams& P, const DevState& S, const double* K, int ns, const double* b,
                     StepCtl* ctl, cudaStream_t st);
+// dt_mode: DT_ADVANCE on stage 4 of the device-resident loop (compute_dt of
+// the stage-4 mesh fused in), -1 otherwise
 void launch_rk4_stage(int nf, const DevParams& P, const DevState& S, int s, const double* mesh_in,
-                      double* mesh_out, double* mesh_zero, long long nzero, StepCtl* ctl, cudaStream_t st);
+                      double* mesh_out, double* mesh_zero, long long nzero, StepCtl* ctl, int dt_mode,
+                      cudaStream_t st);
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
-                            long long* qmesh_out, StepCtl* ctl, cudaStream_t st);
+                            long long* qmesh_out, const long long* qmesh_dt, StepCtl* ctl, int dt_mode,
+                            cudaStream_t st);
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
                            StepCtl* ctl, cudaStream_t st);
 void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st);

@@ -1,0 +1,982 @@
+// emu_kernels.cu -- CUDA kernels (sm_100a) for Emu's per-step evolution path.
+//
+// One thread per particle; particles are cell-sorted so that the lanes of a
+// warp share stencils and their deposits are reduced in registers.
+//   k_rk4_stage<NF,W>        fused RK4 stage (FP64): interpolate the stage
+//                            mesh, -i[H,rho], RK bookkeeping, deposit of the
+//                            next stage state.  Stage 4 also combines, wraps,
+//                            renormalises, deposits the new state for the
+//                            next step and (device-resident loop) reduces
+//                            compute_dt over the stage-4 mesh.
+//   k_rk4_stage_mixed<NF,W>  the same with FP32 interpolation and
+//                            self-interaction commutator, FP64 vacuum+matter
+//                            commutator and state, int64 fixed-point deposit
+//   k_finalize_mixed<NF>     int64 mesh -> FP32 potential mesh
+//   k_dt<NF>                 compute_dt reduction (host-driven calls)
+//   k_deposit / k_rhs / k_stage_state / k_combine: unfused building blocks
+//                            for the C ABI calls and FE/trapezoid/SSPRK3
+// W = stencil widths (WX,WY,WZ): (1,1,3) for 1D runs along z, (3,3,3) for 3D
+// TSC, (0,0,0) generic runtime widths.
+#pragma once
+#include "emu_kernels.cuh"
+
+#include <climits>
+#include <cstdio>
+
+namespace emu {
+
+namespace {
+
+__device__ __constant__ double kRK4A[4] = {0.0, 0.5, 0.5, 1.0};   // a_{s,s-1}
+__device__ __constant__ double kRK4B[4] = {1. / 6., 1. / 3., 1. / 3., 1. / 6.};
+
+inline unsigned grid_for(long long n, int block = kBlock)
+{
+    long long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    return (unsigned)g;
+}
+
+#define STENCIL_LOOP(SWt, BODY)                                  \
+    _Pragma("unroll") for (int kk = 0; kk < SWt::MZ; kk++)       \
+        _Pragma("unroll") for (int jj = 0; jj < SWt::MY; jj++)   \
+            _Pragma("unroll") for (int ii = 0; ii < SWt::MX; ii++) { \
+        if (!SWt::on(P, ii, jj, kk)) continue;                   \
+        BODY                                                     \
+    }
+
+// ---------------------------------------------------------------------------
+// FP64 potential of one particle (Evolve.cpp:163-193 with the Vvac and
+// interpolate fills): V starts at the vacuum term and accumulates
+// coef*inside per stencil cell, nubar with the reference's sign rule.
+template <int NF, class SWt>
+__device__ __forceinline__ void potential_fp64(const DevParams& P, const double* __restrict__ mesh,
+                                               const Stencil<double>& st, double vx, double vy, double vz,
+                                               double vscale, double* V)
+{
+    using H = Herm<NF>;
+    constexpr int NH = NF * NF, ND = 8 * NH;
+#pragma unroll
+    for (int e = 0; e < NH; e++) {
+        V[e] = P.M2[0][e] * vscale;
+        V[NH + e] = P.M2[1][e] * vscale;
+    }
+    STENCIL_LOOP(SWt, {
+        const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
+        const double* __restrict__ m = mesh + cell * ND;
+        const double coef = ((P.sqrt2GF_inv_vol * st.wx[ii]) * st.wy[jj]) * st.wz[kk];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            const double SI = __ldg(m + e) - __ldg(m + 2 * NH + e) * vx - __ldg(m + 4 * NH + e) * vy -
+                              __ldg(m + 6 * NH + e) * vz;
+            const double Sb = __ldg(m + NH + e) - __ldg(m + 3 * NH + e) * vx - __ldg(m + 5 * NH + e) * vy -
+                              __ldg(m + 7 * NH + e) * vz;
+            double inside = H::is_im(e) ? SI + Sb : SI - Sb;
+            if (e == 0) inside = inside + P.matter;
+            const double t = coef * inside;
+            V[e] += t;
+            if (H::is_im(e)) V[NH + e] += t; else V[NH + e] -= t;
+        }
+    })
+}
+
+template <int NF>
+__device__ __forceinline__ void load_state(const double* __restrict__ f, long long cap, long long p, double* out)
+{
+#pragma unroll
+    for (int c = 0; c < 2 * NF * NF; c++) out[c] = f[c * cap + p];
+}
+
+template <int NF>
+__device__ __forceinline__ void store_state(double* __restrict__ f, long long cap, long long p, const double* in)
+{
+#pragma unroll
+    for (int c = 0; c < 2 * NF * NF; c++) f[c * cap + p] = in[c];
+}
+
+// periodic wrap of one coordinate into [0, L) (Redistribute with periodic
+// boundaries).  For x in [-L, 2L) this is the single shift x -/+ L; fmod
+// keeps the cost bounded for any input, and non-finite positions go to 0.
+__device__ __forceinline__ double wrap_coord(double x, double L)
+{
+    if (x >= L || x < 0.0) {
+        if (!isfinite(x)) return 0.0;
+        x = fmod(x, L);
+        if (x < 0.0) x += L;
+        if (x >= L || x < 0.0) x = 0.0;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void report_bad(StepCtl* ctl, int st, long long id)
+{
+    if (st) {
+        atomicOr(&ctl->status, st);
+        atomicMin(&ctl->bad, id);
+    }
+}
+
+// grid-stride zeroing fused into a kernel
+template <class T>
+__device__ __forceinline__ void zero_slice(T* buf, long long n)
+{
+    if (!buf) return;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) buf[i] = (T)0;
+}
+
+// ===========================================================================
+// compute_dt pieces (Evolve.cpp:57-124 + compute_dt fill)
+// ===========================================================================
+__device__ __forceinline__ void block_max2(double& a, double& b)
+{
+    __shared__ double sa[32], sb[32];
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        a = fmax(a, __shfl_xor_sync(kFull, a, off));
+        b = fmax(b, __shfl_xor_sync(kFull, b, off));
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sa[w] = a; sb[w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        a = l < (int)(blockDim.x >> 5) ? sa[l] : 0.0;
+        b = l < (int)(blockDim.x >> 5) ? sb[l] : 0.0;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            a = fmax(a, __shfl_xor_sync(kFull, a, off));
+            b = fmax(b, __shfl_xor_sync(kFull, b, off));
+        }
+    }
+}
+
+template <int NF>
+__device__ __forceinline__ double su_len2_dev(const double* h)
+{
+    using H = Herm<NF>;
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NF; i++)
+#pragma unroll
+        for (int j = i + 1; j < NF; j++) s += h[H::im(i, j)] * h[H::im(i, j)] + h[H::re(i, j)] * h[H::re(i, j)];
+#pragma unroll
+    for (int l = 1; l < NF; l++) {
+        const double cl = (l == 1) ? 0.5 : 0.28867513459481287;
+        double t = 0.0;
+#pragma unroll
+        for (int i = 0; i < l; i++) t += cl * h[H::re(i, i)];
+        t -= cl * l * h[H::re(l, l)];
+        s += t * t;
+    }
+    return s;
+}
+
+// per-cell V_adaptive and V_stupid from the deposited number fields
+template <int NF, class Get>
+__device__ __forceinline__ void cell_potentials(const DevParams& P, Get get, double& Va, double& Vs)
+{
+    using H = Herm<NF>;
+    constexpr int NH = NF * NF;
+    double h[NH];
+#pragma unroll
+    for (int e = 0; e < NH; e++) h[e] = H::is_im(e) ? get(e) + get(NH + e) : get(e) - get(NH + e);
+    h[0] += P.rho * P.Ye / kMp * P.cell_volume;
+    double V2 = su_len2_dev<NF>(h);
+#pragma unroll
+    for (int d = 1; d <= 3; d++) {
+#pragma unroll
+        for (int e = 0; e < NH; e++) h[e] = get(2 * d * NH + e) - get((2 * d + 1) * NH + e);
+        V2 += su_len2_dev<NF>(h);
+    }
+    Va = sqrt(V2) * M_SQRT2 * P.GF / P.cell_volume;
+    double vs = 0.0;
+#pragma unroll
+    for (int i = 0; i < NF; i++) {
+        vs = fmax(vs, get(H::re(i, i)));
+        vs = fmax(vs, get(NH + H::re(i, i)));
+    }
+    vs = fmax(vs, P.cell_volume * P.Ye * P.rho / kMp);
+    Vs = vs * (2.0 * NF * M_SQRT2 * P.GF / P.cell_volume);
+}
+
+// the last block to finish turns the reduced potentials into the next dt
+__device__ void dt_finish(const DevParams& P, StepCtl* ctl, int mode)
+{
+    const double va = __longlong_as_double((long long)ctl->vmax_bits[0]) + P.vvac_max;
+    const double vs = __longlong_as_double((long long)ctl->vmax_bits[1]) + P.vvac_max;
+    double dt_flavor = 0.0;
+    if (P.flavor_cfl_factor > 0.0) {
+        const double dta = kHbar / va * P.flavor_cfl_factor;
+        const double dts = kHbar / vs * P.flavor_cfl_factor;
+        dt_flavor = dts;
+        if (P.max_adaptive_speedup > 1) dt_flavor = fmin(dts * P.max_adaptive_speedup, dta);
+    }
+    double dt = 0.0;
+    const double dtt = P.dt_translation;
+    if (dtt != 0.0 && dt_flavor != 0.0) dt = fmin(dtt, dt_flavor);
+    else if (dtt != 0.0) dt = dtt;
+    else if (dt_flavor != 0.0) dt = dt_flavor;
+    else ctl->status |= ST_DT;
+    if (mode == DT_ADVANCE) {
+        ctl->t = ctl->t + ctl->dt;
+        ctl->step += 1;
+        if (ctl->last || ctl->step >= ctl->max_step) ctl->done = 1;
+    }
+    if (mode != DT_QUERY) {
+        // TimeIntegrator::integrate: clip the step to land on end_time
+        if (ctl->end_time - ctl->t < dt) {
+            dt = ctl->end_time - ctl->t;
+            ctl->last = 1;
+        }
+        if (ctl->status & ST_DT) ctl->done = 1;
+    }
+    ctl->dt = dt;
+    ctl->vmax_bits[0] = 0ull;
+    ctl->vmax_bits[1] = 0ull;
+    ctl->blocks_done = 0u;
+}
+
+template <class T>
+__device__ __forceinline__ double mesh_value(const DevParams& P, const T* m, int q, int NH)
+{
+    return (double)m[q];
+}
+template <>
+__device__ __forceinline__ double mesh_value<long long>(const DevParams& P, const long long* m, int q, int NH)
+{
+    return (double)m[q] * P.q_unscale[(q / NH) & 1];
+}
+
+// Reduce compute_dt over cells [this block's grid-stride share) and, in the
+// last block to arrive, finish the step control.  Every block of the grid
+// must call it exactly once (all threads).  ncb = number of blocks that take
+// part in the cell reduction.
+template <int NF, class T>
+__device__ __forceinline__ void dt_reduce_and_finish(const DevParams& P, const T* __restrict__ mesh, StepCtl* ctl,
+                                                     int mode, unsigned ncb)
+{
+    constexpr int NH = NF * NF, ND = 8 * NH;
+    double va = 0.0, vs = 0.0;
+    if (P.flavor_cfl_factor > 0.0 && blockIdx.x < ncb) {
+        const long long stride = (long long)ncb * blockDim.x;
+        for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.ncells; c += stride) {
+            const T* m = mesh + c * ND;
+            double a, b;
+            cell_potentials<NF>(P, [&](int q) { return mesh_value<T>(P, m, q, NH); }, a, b);
+            va = fmax(va, a);
+            vs = fmax(vs, b);
+        }
+    }
+    block_max2(va, vs);
+    __shared__ bool is_last;
+    if (threadIdx.x == 0) {
+        if (blockIdx.x < ncb) {
+            atomicMax(&ctl->vmax_bits[0], (unsigned long long)__double_as_longlong(va));
+            atomicMax(&ctl->vmax_bits[1], (unsigned long long)__double_as_longlong(vs));
+        }
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->blocks_done, 1u);
+        is_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        dt_finish(P, ctl, mode);
+    }
+}
+
+__device__ __forceinline__ unsigned reduce_blocks(const DevParams& P)
+{
+    long long g = (P.ncells + blockDim.x - 1) / blockDim.x;
+    if (g > 1184) g = 1184;
+    if (g > gridDim.x) g = gridDim.x;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+// ===========================================================================
+// block-level deposit: every thread writes its particle's record to shared
+// memory, then the CTA reduces the records (tile_deposit in emu_device.cuh)
+// ===========================================================================
+template <int NF, class SWt, class R>
+__host__ __device__ constexpr int tile_smem_bytes()
+{
+    return kBlock * 4 + kBlock * TileRec<NF, SWt, R>::RW * (int)sizeof(R);
+}
+
+// int64 fixed-point conversion of a run total (mixed path)
+struct QuantConv {
+    const DevParams& P;
+    __device__ long long operator()(float a, int sp) const
+    {
+        return __float2ll_rn(a * (float)P.q_scale[sp]);
+    }
+};
+
+template <int NF, class SWt, class R, class T, class Conv>
+__device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
+                                                   const R* fN, R vx, R vy, R vz, Conv conv)
+{
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    int* skey = reinterpret_cast<int*>(tile_smem);
+    R* srec = reinterpret_cast<R*>(tile_smem + kBlock * 4);
+    tile_record<NF, SWt, R>(srec, skey, threadIdx.x, active ? stencil_key(P, st.b) : -1, fN, vx, vy, vz, st);
+    __syncthreads();
+    tile_deposit<NF, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
+}
+
+// ===========================================================================
+// fused FP64 RK4 stage
+// ===========================================================================
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S, int s, const double* __restrict__ mesh_in,
+                                                      double* __restrict__ mesh_out, double* mesh_zero, long long nzero,
+                                                      StepCtl* ctl, int dt_mode)
+{
+    using SWt = SW<WX, WY, WZ>;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    if (ctl->done) return;
+    zero_slice(mesh_zero, nzero);
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    const double dt = ctl->dt;
+    const long long cap = S.cap;
+
+    Stencil<double> st{};
+    double fN[NS] = {};
+    double vx = 0, vy = 0, vz = 0;
+    if (active) {
+        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
+        vx = S.vhat[0][p];
+        vy = S.vhat[1][p];
+        vz = S.vhat[2][p];
+        double V[NS];
+        make_stencil<double>(P, x, y, z, st);
+        potential_fp64<NF, SWt>(P, mesh_in, st, vx, vy, vz, S.vscale[p], V);
+        const double bw = dt * kRK4B[s - 1];
+        const double aw = s < 4 ? dt * kRK4A[s] : 0.0;
+        int stt = 0;
+        // one species at a time keeps the live state small
+#pragma unroll
+        for (int sp = 0; sp < 2; sp++) {
+            double f[NH], K[NH];
+#pragma unroll
+            for (int e = 0; e < NH; e++) f[e] = (s == 1 ? S.f0 : S.fs)[(sp * NH + e) * cap + p];
+            commutator<NF, double>(V + sp * NH, f, K, P.inv_hbar);
+            double* fn = f;   // reuse as the next state
+            if (s < 4) {
+#pragma unroll
+                for (int e = 0; e < NH; e++) {
+                    const long long o = (sp * NH + e) * cap + p;
+                    const double y0 = (s == 1) ? f[e] : S.f0[o];
+                    const double a0 = (s == 1) ? y0 : S.acc[o];
+                    S.acc[o] = __dadd_rn(__dmul_rn(bw, K[e]), a0);
+                    fn[e] = __dadd_rn(__dmul_rn(aw, K[e]), y0);
+                    S.fs[o] = fn[e];
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < NH; e++)
+                    fn[e] = __dadd_rn(__dmul_rn(bw, K[e]), S.acc[(sp * NH + e) * cap + p]);
+                stt |= renormalize<NF>(fn, S.Ll[sp][p], P.maxError);
+#pragma unroll
+                for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
+            }
+            const double Ns = S.Nn[sp][p];
+#pragma unroll
+            for (int e = 0; e < NH; e++) fN[sp * NH + e] = fn[e] * Ns;
+        }
+        if (s == 4) {
+            // x, time: the integrator applies the same derivative at every
+            // stage: x += (dt*b_i) * (pup/pupt*c), time += (dt*b_i) * 1
+            double xn[3] = {x, y, z};
+            const double kxv[3] = {vx * kC, vy * kC, vz * kC};
+            double tn = S.time[p];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const double w = dt * kRK4B[i];
+#pragma unroll
+                for (int d = 0; d < 3; d++) xn[d] = __dadd_rn(__dmul_rn(w, kxv[d]), xn[d]);
+                tn = __dadd_rn(w, tn);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                xn[d] = wrap_coord(xn[d], P.L[d]);
+                S.pos[d][p] = xn[d];
+            }
+            S.time[p] = tn;
+            report_bad(ctl, stt, S.id[p]);
+            make_stencil<double>(P, xn[0], xn[1], xn[2], st);
+        }
+    }
+    tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
+                                        [](double a, int) -> double { return a; });
+    // stage 4 of the device-resident loop: compute_dt on the stage-4 mesh
+    // (main.cpp:193-198), which this kernel only reads
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+}
+
+// ===========================================================================
+// unfused building blocks (FP64)
+// ===========================================================================
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_deposit(DevParams P, DevState S, const double* __restrict__ f,
+                                                    double* __restrict__ mesh)
+{
+    using SWt = SW<WX, WY, WZ>;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    Stencil<double> st{};
+    double fN[NS] = {};
+    double vx = 0, vy = 0, vz = 0;
+    if (active) {
+        make_stencil<double>(P, S.pos[0][p], S.pos[1][p], S.pos[2][p], st);
+        vx = S.vhat[0][p];
+        vy = S.vhat[1][p];
+        vz = S.vhat[2][p];
+        const double N0 = S.Nn[0][p], N1 = S.Nn[1][p];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            fN[e] = f[e * S.cap + p] * N0;
+            fN[NH + e] = f[(NH + e) * S.cap + p] * N1;
+        }
+    }
+    tile_deposit_block<NF, SWt, double>(P, mesh, active, st, fN, vx, vy, vz,
+                                        [](double a, int) -> double { return a; });
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_rhs(DevParams P, DevState S, const double* __restrict__ f,
+                                                const double* __restrict__ mesh, double* __restrict__ K)
+{
+    using SWt = SW<WX, WY, WZ>;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    Stencil<double> st;
+    double fl[NS], V[NS], k[NS];
+    load_state<NF>(f, S.cap, p, fl);
+    make_stencil<double>(P, S.pos[0][p], S.pos[1][p], S.pos[2][p], st);
+    potential_fp64<NF, SWt>(P, mesh, st, S.vhat[0][p], S.vhat[1][p], S.vhat[2][p], S.vscale[p], V);
+    commutator<NF, double>(V, fl, k, P.inv_hbar);
+    commutator<NF, double>(V + NH, fl + NH, k + NH, P.inv_hbar);
+    store_state<NF>(K, S.cap, p, k);
+}
+
+// Y = f0; for j: Y = coef_j * K_j + Y   (TimeIntegrator stage state)
+template <int NF>
+__global__ void __launch_bounds__(kBlock) k_stage_state(DevState S, const double* __restrict__ K, int nterms,
+                                                        double c0, double c1, double c2, double* __restrict__ out)
+{
+    constexpr int NS = 2 * NF * NF;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    const double c[3] = {c0, c1, c2};
+    const long long kstride = (long long)NS * S.cap;
+#pragma unroll
+    for (int q = 0; q < NS; q++) {
+        double y = S.f0[q * S.cap + p];
+        for (int j = 0; j < nterms; j++) y = __dadd_rn(__dmul_rn(c[j], K[j * kstride + q * S.cap + p]), y);
+        out[q * S.cap + p] = y;
+    }
+}
+
+// f0 = f0 + sum_i (dt*b_i) K_i ; x, time likewise ; wrap ; Renormalize
+template <int NF>
+__global__ void __launch_bounds__(kBlock) k_combine(DevParams P, DevState S, const double* __restrict__ K, int ns,
+                                                    double w0, double w1, double w2, double w3, StepCtl* ctl)
+{
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    const double w[4] = {w0, w1, w2, w3};
+    const long long kstride = (long long)NS * S.cap;
+    double f[NS];
+#pragma unroll
+    for (int q = 0; q < NS; q++) {
+        double y = S.f0[q * S.cap + p];
+        for (int i = 0; i < ns; i++) y = __dadd_rn(__dmul_rn(w[i], K[i * kstride + q * S.cap + p]), y);
+        f[q] = y;
+    }
+    const double kxv[3] = {S.vhat[0][p] * kC, S.vhat[1][p] * kC, S.vhat[2][p] * kC};
+    double tn = S.time[p];
+    for (int d = 0; d < 3; d++) {
+        double x = S.pos[d][p];
+        for (int i = 0; i < ns; i++) x = __dadd_rn(__dmul_rn(w[i], kxv[d]), x);
+        S.pos[d][p] = wrap_coord(x, P.L[d]);
+    }
+    for (int i = 0; i < ns; i++) tn = __dadd_rn(w[i], tn);
+    S.time[p] = tn;
+    int stt = renormalize<NF>(f, S.Ll[0][p], P.maxError);
+    stt |= renormalize<NF>(f + NH, S.Ll[1][p], P.maxError);
+    report_bad(ctl, stt, S.id[p]);
+    store_state<NF>(S.f0, S.cap, p, f);
+}
+
+template <int NF>
+__global__ void __launch_bounds__(kBlock) k_renorm(DevParams P, DevState S, StepCtl* ctl)
+{
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    double f[NS];
+    load_state<NF>(S.f0, S.cap, p, f);
+    int stt = renormalize<NF>(f, S.Ll[0][p], P.maxError);
+    stt |= renormalize<NF>(f + NH, S.Ll[1][p], P.maxError);
+    report_bad(ctl, stt, S.id[p]);
+    store_state<NF>(S.f0, S.cap, p, f);
+}
+
+// compute_dt for host-driven calls and the initial dt of a run
+template <int NF, class T>
+__global__ void __launch_bounds__(kBlock) k_dt(DevParams P, const T* __restrict__ mesh, StepCtl* ctl, int mode)
+{
+    if (mode == DT_ADVANCE && ctl->done) return;
+    dt_reduce_and_finish<NF, T>(P, mesh, ctl, mode, gridDim.x);
+}
+
+// ===========================================================================
+// mixed precision
+// ===========================================================================
+// finalize an int64 mesh into FP32 potentials G[cell][d][e] =
+// sqrt(2)GF/dV * (M_d,nu,e + sgn_e M_d,nubar,e) and zero the other int64
+// mesh (the one the next stage deposits into).
+template <int NF>
+__global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const long long* __restrict__ q,
+                                                           long long* __restrict__ qzero, float* __restrict__ g,
+                                                           StepCtl* ctl)
+{
+    using H = Herm<NF>;
+    constexpr int NH = NF * NF, ND = 8 * NH;
+    if (ctl->done) return;
+    zero_slice(qzero, qzero ? P.ncells * ND : 0);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.ncells; c += stride) {
+        const long long* m = q + c * ND;
+#pragma unroll
+        for (int d = 0; d < 4; d++)
+#pragma unroll
+            for (int e = 0; e < NH; e++) {
+                const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
+                const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
+                const double comb = H::is_im(e) ? a + b : a - b;
+                g[c * 4 * NH + d * NH + e] = (float)(P.sqrt2GF_inv_vol * comb);
+            }
+    }
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_deposit_q(DevParams P, DevState S, const double* __restrict__ f,
+                                                      long long* __restrict__ mesh)
+{
+    using SWt = SW<WX, WY, WZ>;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    Stencil<float> st{};
+    float fN[NS] = {};
+    float vx = 0, vy = 0, vz = 0;
+    if (active) {
+        make_stencil<float>(P, S.pos[0][p], S.pos[1][p], S.pos[2][p], st);
+        vx = S.vhat32[0][p];
+        vy = S.vhat32[1][p];
+        vz = S.vhat32[2][p];
+        const float N0 = S.N32[0][p], N1 = S.N32[1][p];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            fN[e] = (float)f[e * S.cap + p] * N0;
+            fN[NH + e] = (float)f[(NH + e) * S.cap + p] * N1;
+        }
+    }
+    tile_deposit_block<NF, SWt, float>(P, mesh, active, st, fN, vx, vy, vz, QuantConv{P});
+}
+
+// FP32 self-interaction potential from the finalized mesh: H_SI,e (nu); the
+// nubar potential is sgn_e * H_SI,e (generate_code.py:317-355)
+template <int NF, class SWt>
+__device__ __forceinline__ void potential_si32(const DevParams& P, const float* __restrict__ g, const Stencil<float>& st,
+                                               float vx, float vy, float vz, float* hs)
+{
+    constexpr int NH = NF * NF;
+#pragma unroll
+    for (int e = 0; e < NH; e++) hs[e] = 0.f;
+    STENCIL_LOOP(SWt, {
+        const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
+        // the cell's 4*NH potentials, 16-byte vector loads (cell stride 64 or 144 bytes)
+        const float4* __restrict__ m4 = reinterpret_cast<const float4*>(g + cell * 4 * NH);
+        float m[4 * NH];
+#pragma unroll
+        for (int k = 0; k < NH; k++) {
+            const float4 v = __ldg(m4 + k);
+            m[4 * k] = v.x; m[4 * k + 1] = v.y; m[4 * k + 2] = v.z; m[4 * k + 3] = v.w;
+        }
+        const float w = st.wx[ii] * st.wy[jj] * st.wz[kk];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            const float v = m[e] - m[NH + e] * vx - m[2 * NH + e] * vy - m[3 * NH + e] * vz;
+            hs[e] = fmaf(w, v, hs[e]);
+        }
+    })
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevState S, int s,
+                                                            const float* __restrict__ gmesh,
+                                                            long long* __restrict__ qout,
+                                                            const long long* __restrict__ qdt, StepCtl* ctl,
+                                                            int dt_mode)
+{
+    using H = Herm<NF>;
+    using SWt = SW<WX, WY, WZ>;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    if (ctl->done) return;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    const double dt = ctl->dt;
+    const long long cap = S.cap;
+
+    Stencil<float> st{};
+    float fN[NS] = {};
+    float vx = 0, vy = 0, vz = 0;
+    if (active) {
+        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
+        vx = S.vhat32[0][p];
+        vy = S.vhat32[1][p];
+        vz = S.vhat32[2][p];
+        make_stencil<float>(P, x, y, z, st);
+        // FP32 self-interaction part, trace removed (it commutes)
+        float hs[NH];
+        potential_si32<NF, SWt>(P, gmesh, st, vx, vy, vz, hs);
+        float tr = 0.f;
+#pragma unroll
+        for (int i = 0; i < NF; i++) tr += hs[H::re(i, i)];
+        tr *= (1.0f / NF);
+#pragma unroll
+        for (int e = 0; e < NH; e++)
+            if (H::is_diag(e)) hs[e] -= tr;
+        const float ih = (float)P.inv_hbar;
+        const double vs = S.vscale[p];
+        const double mat = P.sqrt2GF_inv_vol * P.matter;
+        const double aw = s > 1 ? dt * kRK4A[s - 1] : 0.0;
+        const double an = s < 4 ? dt * kRK4A[s] : 0.0;
+        const double w6 = dt * (1.0 / 6.0);
+        int stt = 0;
+        // one species at a time keeps the live state small
+#pragma unroll
+        for (int sp = 0; sp < 2; sp++) {
+            double y0[NH], f[NH];
+#pragma unroll
+            for (int e = 0; e < NH; e++) {
+                const long long o = (sp * NH + e) * cap + p;
+                y0[e] = S.f0[o];
+                f[e] = s > 1 ? y0[e] + aw * (double)S.k32[o] : y0[e];
+            }
+            // nubar: H_SI conjugated and negated (generate_code.py:317-355)
+            float hsn[NH], f32[NH], ksi[NH];
+#pragma unroll
+            for (int e = 0; e < NH; e++) {
+                hsn[e] = (sp == 0 || H::is_im(e)) ? hs[e] : -hs[e];
+                f32[e] = (float)f[e];
+            }
+            commutator<NF, float>(hsn, f32, ksi, ih);
+            // FP64 vacuum + matter part
+            double Hv[NH], Kv[NH];
+#pragma unroll
+            for (int e = 0; e < NH; e++) Hv[e] = P.M2[sp][e] * vs;
+            Hv[0] += sp == 0 ? mat : -mat;
+            commutator<NF, double>(Hv, f, Kv, P.inv_hbar);
+            double fn[NH];
+            if (s < 4) {
+#pragma unroll
+                for (int e = 0; e < NH; e++) {
+                    const long long o = (sp * NH + e) * cap + p;
+                    const float kc = (float)(Kv[e] + (double)ksi[e]);
+                    S.k32[o] = kc;
+                    S.ksum32[o] = (s == 1) ? kc : fmaf(2.f, kc, S.ksum32[o]);
+                    fn[e] = y0[e] + an * (double)kc;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < NH; e++) {
+                    const long long o = (sp * NH + e) * cap + p;
+                    fn[e] = y0[e] + w6 * ((double)S.ksum32[o] + (Kv[e] + (double)ksi[e]));
+                }
+                stt |= renormalize<NF>(fn, S.Ll[sp][p], P.maxError);
+#pragma unroll
+                for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
+            }
+            const float Ns = S.N32[sp][p];
+#pragma unroll
+            for (int e = 0; e < NH; e++) fN[sp * NH + e] = (float)fn[e] * Ns;
+        }
+        if (s == 4) {
+            double xn[3] = {x, y, z};
+            double tn = S.time[p];
+            const double ipt = 1.0 / S.pup[3][p];
+            const double kxv[3] = {S.pup[0][p] * ipt * kC, S.pup[1][p] * ipt * kC, S.pup[2][p] * ipt * kC};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const double w = dt * kRK4B[i];
+#pragma unroll
+                for (int d = 0; d < 3; d++) xn[d] = __dadd_rn(__dmul_rn(w, kxv[d]), xn[d]);
+                tn = __dadd_rn(w, tn);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                xn[d] = wrap_coord(xn[d], P.L[d]);
+                S.pos[d][p] = xn[d];
+            }
+            S.time[p] = tn;
+            report_bad(ctl, stt, S.id[p]);
+            make_stencil<float>(P, xn[0], xn[1], xn[2], st);
+        }
+    }
+    tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P});
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
+}
+
+// ===========================================================================
+// data movement
+// ===========================================================================
+// AoS records (rows of 3+nattribs) -> SoA, row perm[i] goes to slot i
+template <int NF>
+__global__ void k_pack(DevParams P, const double* __restrict__ aos, const unsigned* __restrict__ perm, long long n,
+                       DevState S)
+{
+    constexpr int NH = NF * NF, NA = 8 + 2 * (2 + NH), NR = 3 + NA;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long row = perm ? (long long)perm[i] : i;
+    const double* r = aos + row * NR;
+    for (int d = 0; d < 3; d++) S.pos[d][i] = r[d];
+    S.time[i] = r[3 + 0];
+    for (int d = 0; d < 4; d++) S.pup[d][i] = r[3 + 4 + d];
+    const double pupt = r[3 + 7];
+    for (int d = 0; d < 3; d++) S.vhat[d][i] = r[3 + 4 + d] / pupt;
+    S.vscale[i] = P.c4 / (2. * pupt);
+    for (int sp = 0; sp < 2; sp++) {
+        const int base = 3 + 8 + sp * (2 + NH);
+        S.Nn[sp][i] = r[base];
+        S.Ll[sp][i] = r[base + 1];
+        for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * S.cap + i] = r[base + 2 + e];
+    }
+    S.id[i] = row;
+}
+
+template <int NF>
+__global__ void k_unpack(DevState S, double* __restrict__ aos)
+{
+    constexpr int NH = NF * NF, NA = 8 + 2 * (2 + NH), NR = 3 + NA;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    double* r = aos + S.id[i] * NR;
+    for (int d = 0; d < 3; d++) {
+        r[d] = S.pos[d][i];
+        r[3 + 1 + d] = S.pos[d][i];
+    }
+    r[3] = S.time[i];
+    for (int d = 0; d < 4; d++) r[3 + 4 + d] = S.pup[d][i];
+    for (int sp = 0; sp < 2; sp++) {
+        const int base = 3 + 8 + sp * (2 + NH);
+        r[base] = S.Nn[sp][i];
+        r[base + 1] = S.Ll[sp][i];
+        for (int e = 0; e < NH; e++) r[base + 2 + e] = S.f0[(sp * NH + e) * S.cap + i];
+    }
+}
+
+// derivative records (interpolate_rhs_from_mesh output, Evolve.cpp:195-210)
+template <int NF>
+__global__ void k_unpack_rhs(DevState S, const double* __restrict__ K, double* __restrict__ aos)
+{
+    constexpr int NH = NF * NF, NA = 8 + 2 * (2 + NH), NR = 3 + NA;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    double* r = aos + S.id[i] * NR;
+    for (int d = 0; d < 3; d++) r[d] = S.pos[d][i];
+    for (int a = 0; a < NA; a++) r[3 + a] = 0.0;
+    r[3 + 0] = 1.0;
+    for (int d = 0; d < 3; d++) r[3 + 1 + d] = S.pup[d][i] / S.pup[3][i] * kC;
+    for (int sp = 0; sp < 2; sp++) {
+        const int base = 3 + 8 + sp * (2 + NH);
+        for (int e = 0; e < NH; e++) r[base + 2 + e] = K[(sp * NH + e) * S.cap + i];
+    }
+}
+
+__global__ void k_cell_keys_aos(DevParams P, const double* __restrict__ aos, int nreal, long long n,
+                                unsigned* keys, unsigned* idx)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Stencil<double> st;
+    make_stencil<double>(P, aos[i * nreal + 0], aos[i * nreal + 1], aos[i * nreal + 2], st);
+    keys[i] = (unsigned)stencil_key(P, st.b);
+    idx[i] = (unsigned)i;
+}
+
+__global__ void k_cell_keys_soa(DevParams P, DevState S, unsigned* keys, unsigned* idx)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    Stencil<double> st;
+    make_stencil<double>(P, S.pos[0][i], S.pos[1][i], S.pos[2][i], st);
+    keys[i] = (unsigned)stencil_key(P, st.b);
+    idx[i] = (unsigned)i;
+}
+
+template <int NF>
+__global__ void k_gather_state(DevState src, DevState dst, const unsigned* __restrict__ perm, int mixed)
+{
+    constexpr int NS = 2 * NF * NF;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= src.n) return;
+    const long long j = perm[i];
+    for (int d = 0; d < 3; d++) { dst.pos[d][i] = src.pos[d][j]; dst.vhat[d][i] = src.vhat[d][j]; }
+    dst.time[i] = src.time[j];
+    for (int d = 0; d < 4; d++) dst.pup[d][i] = src.pup[d][j];
+    for (int sp = 0; sp < 2; sp++) { dst.Nn[sp][i] = src.Nn[sp][j]; dst.Ll[sp][i] = src.Ll[sp][j]; }
+    dst.vscale[i] = src.vscale[j];
+    dst.id[i] = src.id[j];
+    for (int c = 0; c < NS; c++) dst.f0[c * dst.cap + i] = src.f0[c * src.cap + j];
+    if (mixed) {
+        for (int d = 0; d < 3; d++) dst.vhat32[d][i] = src.vhat32[d][j];
+        for (int sp = 0; sp < 2; sp++) dst.N32[sp][i] = src.N32[sp][j];
+    }
+}
+
+__global__ void k_mixed_shadow(DevState S)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    for (int d = 0; d < 3; d++) S.vhat32[d][i] = (float)S.vhat[d][i];
+    for (int sp = 0; sp < 2; sp++) S.N32[sp][i] = (float)S.Nn[sp][i];
+}
+
+template <int NF>
+__global__ void k_mesh_out(DevParams P, const double* __restrict__ mesh, double* __restrict__ out)
+{
+    constexpr int ND = 8 * NF * NF;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.ncells * ND) return;
+    const long long c = i / ND;
+    const int q = (int)(i % ND);
+    out[(3 + q) * P.ncells + c] = mesh[i];
+}
+
+template <int NF>
+__global__ void k_mesh_out_q(DevParams P, const long long* __restrict__ mesh, double* __restrict__ out)
+{
+    constexpr int NH = NF * NF, ND = 8 * NH;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.ncells * ND) return;
+    const long long c = i / ND;
+    const int q = (int)(i % ND);
+    out[(3 + q) * P.ncells + c] = (double)mesh[i] * P.q_unscale[(q / NH) & 1];
+}
+
+template <int NF>
+__global__ void k_q_to_f64(DevParams P, const long long* __restrict__ mesh, double* __restrict__ out)
+{
+    constexpr int NH = NF * NF, ND = 8 * NH;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.ncells * ND) return;
+    out[i] = (double)mesh[i] * P.q_unscale[((int)(i % ND) / NH) & 1];
+}
+
+__global__ void k_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status)
+{
+    ctl->dt = dt;
+    ctl->t = t;
+    ctl->end_time = end_time;
+    ctl->done = max_step <= 0 ? 1 : 0;
+    ctl->step = 0;
+    ctl->max_step = max_step;
+    ctl->last = 0;
+    ctl->blocks_done = 0u;
+    ctl->vmax_bits[0] = ctl->vmax_bits[1] = 0ull;
+    if (reset_status) {
+        ctl->status = 0;
+        ctl->bad = LLONG_MAX;
+    }
+}
+
+__global__ void k_flush(double* buf, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) buf[i] = buf[i] * 0.5 + 1.0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// launcher templates (explicitly instantiated per flavor count in
+// emu_k_fp64_<nf>.cu / emu_k_mixed_<nf>.cu, dispatched in emu_kernels.cu)
+// ===========================================================================
+inline unsigned launch_grid(long long n) { return grid_for(n); }
+
+// stencil-width specialisations: 1D along z with TSC, 3D TSC, generic
+#define EMU_W_DISPATCH(P, KERNEL_CALL)                                            \
+    do {                                                                          \
+        if ((P).w[0] == 1 && (P).w[1] == 1 && (P).w[2] == 3) {                    \
+            constexpr int WXv = 1, WYv = 1, WZv = 3;                              \
+            KERNEL_CALL;                                                          \
+        } else if ((P).w[0] == 3 && (P).w[1] == 3 && (P).w[2] == 3) {             \
+            constexpr int WXv = 3, WYv = 3, WZv = 3;                              \
+            KERNEL_CALL;                                                          \
+        } else {                                                                  \
+            constexpr int WXv = 0, WYv = 0, WZv = 0;                              \
+            KERNEL_CALL;                                                          \
+        }                                                                         \
+    } while (0)
+
+// tiles above the 48 KB default need the opt-in attribute (FP64, 3 flavors,
+// 27-cell stencils: 51 KB)
+template <class K>
+void smem_optin(K kernel, int bytes)
+{
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <int NF>
+void launch_rk4_stage_t(const DevParams& P, const DevState& S, int s, const double* mesh_in, double* mesh_out,
+                        double* mesh_zero, long long nzero, StepCtl* ctl, int dt_mode, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        smem_optin(k_rk4_stage<NF, WXv, WYv, WZv>, bytes);
+        k_rk4_stage<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, s, mesh_in, mesh_out, mesh_zero,
+                                                                            nzero, ctl, dt_mode);
+    });
+}
+
+template <int NF>
+void launch_deposit_t(const DevParams& P, const DevState& S, const double* f, double* mesh, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        smem_optin(k_deposit<NF, WXv, WYv, WZv>, bytes);
+        k_deposit<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, f, mesh);
+    });
+}
+
+template <int NF>
+void launch_rhs_t(const DevParams& P, const DevState& S, const double* f, const double* mesh, double* K,
+                  cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, (k_rhs<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, 0, st>>>(P, S, f, mesh, K)));
+}
+
+template <int NF>
+void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, const float* gmesh, long long* qout,
+                              const long long* qdt, StepCtl* ctl, int dt_mode, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, (k_rk4_stage_mixed<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>(), st>>>(
+                          P, S, s, gmesh, qout, qdt, ctl, dt_mode)));
+}
+
+template <int NF>
+void launch_deposit_q_t(const DevParams& P, const DevState& S, const double* f, long long* mesh, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, (k_deposit_q<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>(), st>>>(P, S, f, mesh)));
+}
+
+}  // namespace emu

@@ -37,6 +37,23 @@ def mesh_rel(a, b, ncomp):
     return colwise_rel(a.reshape(ncomp, -1).T, b.reshape(ncomp, -1).T)
 
 
+def magnitude_mesh(oracle, parts):
+    """Per-cell, per-component sum of |contribution| (the deposit of |f| N
+    |v|): the scale that rounding errors of a deposit are relative to."""
+    q = np.array(parts, dtype=np.float64, copy=True)
+    q[:, 3:] = np.abs(q[:, 3:])
+    return oracle.deposit(q)
+
+
+def mesh_rel_mag(a, b, mag, ncomp):
+    """max over components of max|a-b| / max(magnitude) of that component"""
+    a = a.reshape(ncomp, -1)[3:]
+    b = b.reshape(ncomp, -1)[3:]
+    m = np.abs(mag.reshape(ncomp, -1)[3:]).max(axis=1)
+    err = np.abs(a - b).max(axis=1)
+    return float((err / np.maximum(m, 1e-300)).max())
+
+
 def flavor_cols(nf):
     nh = nf * nf
     return list(range(3 + 10, 3 + 10 + nh)) + list(range(3 + 12 + nh, 3 + 12 + 2 * nh))

@@ -11,7 +11,8 @@ import pytest
 from emu_b200 import api
 from emu_b200 import workloads as W
 from oracle.oracle import Oracle
-from tests.helpers import GOLDEN, colwise_rel, flavor_cols, golden_ids, load_golden, mesh_rel
+from tests.helpers import (GOLDEN, colwise_rel, flavor_cols, golden_ids, load_golden, magnitude_mesh, mesh_rel,
+                           mesh_rel_mag)
 
 pytestmark = pytest.mark.gpu
 
@@ -125,7 +126,9 @@ def test_step_api_sequence_matches_oracle():
             mesh, s, _ = o.rk_step(q, dt_o)
             c.step(dt_o)
         assert colwise_rel(c.get_particles(), q) < 1e-11
-        assert mesh_rel(c.get_mesh(), mesh, 75) < 1e-11
+        # Fz00 of the isotropic nu field cancels to rounding level: compare
+        # against the magnitude of the deposited terms
+        assert mesh_rel_mag(c.get_mesh(), mesh, magnitude_mesh(o, q), 75) < 1e-13
 
 
 def test_single_particle_and_edges():
