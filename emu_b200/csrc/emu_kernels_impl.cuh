@@ -914,17 +914,17 @@ __global__ void k_flush(double* buf, long long n)
 inline unsigned launch_grid(long long n) { return grid_for(n); }
 
 // stencil-width specialisations: 1D along z with TSC, 3D TSC, generic
-#define EMU_W_DISPATCH(P, KERNEL_CALL)                                            \
+#define EMU_W_DISPATCH(P, ...)                                                    \
     do {                                                                          \
         if ((P).w[0] == 1 && (P).w[1] == 1 && (P).w[2] == 3) {                    \
             constexpr int WXv = 1, WYv = 1, WZv = 3;                              \
-            KERNEL_CALL;                                                          \
+            __VA_ARGS__;                                                          \
         } else if ((P).w[0] == 3 && (P).w[1] == 3 && (P).w[2] == 3) {             \
             constexpr int WXv = 3, WYv = 3, WZv = 3;                              \
-            KERNEL_CALL;                                                          \
+            __VA_ARGS__;                                                          \
         } else {                                                                  \
             constexpr int WXv = 0, WYv = 0, WZv = 0;                              \
-            KERNEL_CALL;                                                          \
+            __VA_ARGS__;                                                          \
         }                                                                         \
     } while (0)
 
