@@ -128,6 +128,8 @@ SIGNATURES = {
     "emu_read_particles": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _D, ctypes.c_int64,
                                           _P(ctypes.c_int64), _D, _P(ctypes.c_int)]),
     "emu_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "emu_deposit_noalloc": (ctypes.c_int, [_P(EmuParams), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
 }
 
 

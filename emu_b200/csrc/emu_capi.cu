@@ -78,9 +78,13 @@ int check_launch(emu_context* ctx, const char* what)
 
 int widths(int ord) { return ord >= 2 ? 3 : (ord == 1 ? 2 : 1); }
 
+}  // namespace
+
+void emu_host::set_error(const std::string& msg) { g_host_err = msg; }
+
 // DevParams from the run parameters (geometry as AMReX computes it:
 // CellSize = L/n, InvCellSize = 1/CellSize)
-void make_devparams(const emu_params& p, DevParams& P)
+void emu::make_devparams(const emu_params& p, DevParams& P)
 {
     std::memset(&P, 0, sizeof(P));
     P.nf = p.nflavors;
@@ -118,6 +122,8 @@ void make_devparams(const emu_params& p, DevParams& P)
     P.q_scale[0] = P.q_scale[1] = 1.0;
     P.q_unscale[0] = P.q_unscale[1] = 1.0;
 }
+
+namespace {
 
 template <class T>
 T* carve(char*& ptr, long long count)
@@ -461,7 +467,7 @@ int emu_create(const emu_params* p, emu_context** out)
     ctx->ND = 8 * ctx->NH;
     ctx->nreal = emu_nreal(ctx->nf);
     ctx->mixed = p->precision == EMU_PREC_MIXED;
-    make_devparams(*p, ctx->P);
+    emu::make_devparams(*p, ctx->P);
     int r = EMU_OK;
     auto bail = [&](int code) {
         g_host_err = ctx->err;

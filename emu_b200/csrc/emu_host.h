@@ -17,6 +17,9 @@ double gf();
 
 bool validate(const emu_params& p, std::string& why);
 
+// message returned by emu_last_error(NULL, ...)
+void set_error(const std::string& msg);
+
 // flavour-basis mass-squared matrix in Hermitian component order for nu
 // (m2[0]) and nubar (m2[1], conjugated), generate_code.py:174-255
 void vacuum_m2(const emu_params& p, double m2[2][9]);

@@ -16,7 +16,12 @@
 
 #include "emu_device.cuh"
 
+struct emu_params;
+
 namespace emu {
+
+// kernel parameters from the run parameters (emu_capi.cu)
+void make_devparams(const emu_params& p, DevParams& P);
 
 struct DevState {
     long long n = 0, cap = 0;

@@ -207,6 +207,32 @@ int emu_read_particles(const char* plotfile_dir, int nflavors, double* out, int6
  * when ctx is NULL). */
 int emu_last_error(const emu_context* ctx, char* buf, size_t len);
 
+/*
+ * deposit_to_mesh for callers that cannot allocate device memory.  No
+ * counterpart in the reference: its deposit writes into an AMReX MultiFab
+ * the caller already owns.  Some callers cannot call cudaMalloc when they
+ * need a deposit (work being captured into a CUDA graph, a fixed memory pool
+ * handed over at start-up, a loop that must not touch the allocator); this
+ * entry point allocates nothing.  Inputs and outputs are device memory owned
+ * by the caller:
+ *   d_records   n particle records (rows of emu_nreal(nflavors) FP64, the
+ *               emu_load_particles layout), on the device
+ *   d_mesh_out  emu_ncomp(nflavors) x ncells FP64 in emu_get_mesh layout
+ * Its only scratch, the cell-major accumulation mesh, is a fixed array of
+ * 2^19 doubles (4 MiB) compiled into the library; ncells * 8 * nflavors^2
+ * must not exceed it (EMU_ERR_LIMIT otherwise).  Every GPU that loads the
+ * library keeps the array until the process exits.  The first call on a
+ * device looks up the array's device address once (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  All calls share the
+ * array and each call clears it first, so calls that overlap on the GPU
+ * (different streams, threads or processes on one device) race and must be
+ * serialised by the caller.  Work is enqueued on `stream` (a cudaStream_t,
+ * NULL = the legacy default stream); the call does not synchronise.
+ * Errors: emu_last_error(NULL, ...).
+ */
+int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n, double* d_mesh_out,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif
