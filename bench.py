@@ -39,7 +39,7 @@ from emu_b200 import workloads as W  # noqa: E402
 METRIC = "particle RK4 steps/s on 1 B200: mixed vs FP64 at stated err; % of HBM peak"
 
 
-def workload(name, precision, cells=None):
+def workload(name, precision, cells=None, fused=None):
     """cells overrides the cell count (z cells for c2/c3, cells per side for
     c5) to run a smaller case of the same workload (profiling)."""
     if name == "c2":
@@ -56,6 +56,8 @@ def workload(name, precision, cells=None):
         raise SystemExit("unknown workload " + name)
     if precision:
         p.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
+    if fused:
+        p.fused = fused
     return p, desc
 
 
@@ -164,7 +166,7 @@ def run_reference(args):
     ws, rank, local = dist_setup(args)
     if rank != 0:
         return
-    p, desc = workload(args.workload, args.precision, args.cells)
+    p, desc = workload(args.workload, args.precision, args.cells, args.fused)
     recs = api.init_particles(p)
     nthreads = os.cpu_count() or 1
     from oracle.oracle import Oracle, RefHarness, have_ref
@@ -209,7 +211,7 @@ def run_emu(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    p, desc = workload(args.workload, args.precision, args.cells)
+    p, desc = workload(args.workload, args.precision, args.cells, args.fused)
     mixed = p.precision == api.PREC_MIXED
     nf = p.nflavors
     recs = api.init_particles(p)
@@ -260,10 +262,18 @@ def run_emu(args):
         ctx.flush_l2(flush.data_ptr(), flush_bytes)
         kms.append(ctx.profile_step())
     kms = np.array(kms)
-    stage_idx = [1, 3, 5, 7] if mixed else [0, 1, 2, 3]
-    stage_ms = float(kms[:, stage_idx].mean())
     per_pstep = algorithmic_bytes_per_particle_step(nf, mixed)
-    bytes_per_launch = (per_pstep * n + mesh_bytes_per_step(p, nf)) / 4.0
+    coop = kms.shape[1] == 1
+    if coop:
+        # one cooperative kernel per step: the whole step is the launch
+        kernel = "k_rk4_step_coop<%d>" % nf
+        stage_ms = float(kms[:, 0].mean())
+        bytes_per_launch = per_pstep * n + mesh_bytes_per_step(p, nf)
+    else:
+        kernel = "k_rk4_stage%s<%d>" % ("_mixed" if mixed else "", nf)
+        stage_idx = [1, 3, 5, 7] if mixed else [0, 1, 2, 3]
+        stage_ms = float(kms[:, stage_idx].mean())
+        bytes_per_launch = (per_pstep * n + mesh_bytes_per_step(p, nf)) / 4.0
     peak, peak_kind = load_peaks()
     achieved = bytes_per_launch / (stage_ms * 1e-3) / 1e9
     traffic = None
@@ -300,7 +310,7 @@ def run_emu(args):
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(p, recs, args.cpu_budget, os.cpu_count() or 1)
 
-    kernels_per_step = 9 if mixed else 5
+    kernels_per_step = 1 if coop else (8 if mixed else 4)
     resorts = (args.steps // p.resort_interval) if p.resort_interval > 0 else 0
     out = {
         "metric": METRIC,
@@ -322,7 +332,7 @@ def run_emu(args):
                    "resort_interval": p.resort_interval},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "k_rk4_stage%s<%d>" % ("_mixed" if mixed else "", nf),
+                     "kernel": kernel,
                      "kernel_ms": stage_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
                      "peak_source": peak_kind},
         "e2e": e2e,
@@ -348,6 +358,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"])
     ap.add_argument("--cells", type=int, default=None, help="smaller case of the workload (cells per side)")
+    ap.add_argument("--fused", type=int, default=None, choices=[1, 2],
+                    help="RK4 kernels: 2 one cooperative launch per step when it fits (default), 1 per stage")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=15.0)

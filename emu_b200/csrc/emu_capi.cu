@@ -49,6 +49,7 @@ struct emu_context {
     bool loaded = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int steps_since_sort = 0;
+    bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
     std::string err;
 };
 
@@ -579,6 +580,8 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     if (ctx->mixed) emu::launch_mixed_shadow(ctx->nf, S, ctx->stream);
     if ((r = check_launch(ctx, "pack"))) return r;
     free_graphs(ctx);   // kernel arguments (P, S) changed
+    // fused == 2 (default): one cooperative launch per step when the grid fits
+    ctx->coop = !ctx->mixed && ctx->prm.fused == 2 && rk4_fused(ctx) && emu::coop_step_fits(ctx->nf, ctx->P, n);
     ctx->loaded = true;
     ctx->steps_since_sort = 0;
     if ((r = deposit_current(ctx))) return r;
@@ -703,7 +706,15 @@ int emu_step(emu_context* ctx, double dt, int64_t* bad)
     emu::launch_ctl_set(ctx->ctl, dt, 0.0, INFINITY, 1, 1, ctx->stream);
     if (rk4_fused(ctx)) {
         if (!ctx->fused_ready && (r = deposit_current(ctx))) return r;
-        r = ctx->mixed ? enqueue_rk4_mixed(ctx, ctx->stream, false) : enqueue_rk4_fp64(ctx, ctx->stream, false);
+        if (ctx->coop) {
+            double* const m[4] = {ctx->mesh[0], ctx->mesh[1], ctx->mesh[2], ctx->mesh[3]};
+            cudaError_t e = emu::launch_rk4_step_coop(ctx->nf, ctx->P, ctx->S[ctx->cur], m, mesh_elems(ctx), ctx->ctl,
+                                                      -1, ctx->stream);
+            r = e == cudaSuccess ? EMU_OK : fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") +
+                                                                      cudaGetErrorString(e));
+        } else {
+            r = ctx->mixed ? enqueue_rk4_mixed(ctx, ctx->stream, false) : enqueue_rk4_fp64(ctx, ctx->stream, false);
+        }
         if (r) return r;
         ctx->cur_mesh = ctx->mixed ? 1 : 3;
         ctx->fused_ready = true;
@@ -735,8 +746,16 @@ int emu_evolve_steps(emu_context* ctx, int nsteps)
     if (!ctx) return EMU_ERR_ARG;
     int r;
     for (int i = 0; i < nsteps; i++) {
-        if (!ctx->graph[ctx->cur] && (r = build_graph(ctx))) return r;
-        CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        if (ctx->coop) {
+            double* const m[4] = {ctx->mesh[0], ctx->mesh[1], ctx->mesh[2], ctx->mesh[3]};
+            cudaError_t e = emu::launch_rk4_step_coop(ctx->nf, ctx->P, ctx->S[ctx->cur], m, mesh_elems(ctx),
+                                                      ctx->ctl, emu::DT_ADVANCE, ctx->stream);
+            if (e != cudaSuccess)
+                return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
+        } else {
+            if (!ctx->graph[ctx->cur] && (r = build_graph(ctx))) return r;
+            CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        }
         ctx->cur_mesh = ctx->mixed ? 1 : 3;
         if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
             if ((r = resort(ctx))) return r;
@@ -779,6 +798,29 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
 {
     if (!ctx || !kernel_ms || !nkernels) return EMU_ERR_ARG;
     if (!rk4_fused(ctx)) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: requires fused RK4");
+    if (ctx->coop) {
+        // one cooperative kernel per step
+        if (max_kernels < 1) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
+        cudaEvent_t a, b;
+        CU(cudaEventCreate(&a));
+        CU(cudaEventCreate(&b));
+        double* const m[4] = {ctx->mesh[0], ctx->mesh[1], ctx->mesh[2], ctx->mesh[3]};
+        CU(cudaEventRecord(a, ctx->stream));
+        cudaError_t e = emu::launch_rk4_step_coop(ctx->nf, ctx->P, ctx->S[ctx->cur], m, mesh_elems(ctx), ctx->ctl,
+                                                  emu::DT_ADVANCE, ctx->stream);
+        CU(cudaEventRecord(b, ctx->stream));
+        if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
+        CU(cudaEventSynchronize(b));
+        CU(cudaEventElapsedTime(&kernel_ms[0], a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        *nkernels = 1;
+        ctx->cur_mesh = 3;
+        int r;
+        if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
+            if ((r = resort(ctx))) return r;
+        return EMU_OK;
+    }
     const int nk = ctx->mixed ? 8 : 4;
     if (max_kernels < nk) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
     std::vector<cudaEvent_t> ev(2 * nk);

@@ -26,7 +26,7 @@ constexpr double kEV = 1.60218e-12;
 constexpr unsigned kFull = 0xffffffffu;
 
 // status bits shared with include/emu_b200.h
-enum : int { ST_TRACE = 1, ST_NEGDIAG = 2, ST_LENGTH = 4, ST_DT = 8 };
+enum : int { ST_TRACE = 1, ST_NEGDIAG = 2, ST_LENGTH = 4, ST_DT = 8, ST_TIMEOUT = 2048 };
 
 // ---------------------------------------------------------------------------
 // Hermitian component layout: upper triangle, row-major, Re before Im

@@ -7,4 +7,7 @@ template void launch_rk4_stage_t<3>(const DevParams&, const DevState&, int, cons
 template void launch_deposit_t<3>(const DevParams&, const DevState&, const double*, double*, cudaStream_t);
 template void launch_rhs_t<3>(const DevParams&, const DevState&, const double*, const double*, double*,
                               cudaStream_t);
+template bool coop_step_fits_t<3>(const DevParams&, long long);
+template cudaError_t launch_rk4_step_coop_t<3>(const DevParams&, const DevState&, double* const*, long long,
+                                               StepCtl*, int, cudaStream_t);
 }  // namespace emu

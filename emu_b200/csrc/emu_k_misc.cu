@@ -16,7 +16,10 @@ namespace emu {
     extern template void launch_rk4_stage_mixed_t<NF>(const DevParams&, const DevState&, int, const float*,      \
                                                       long long*, const long long*, StepCtl*, int, cudaStream_t); \
     extern template void launch_deposit_q_t<NF>(const DevParams&, const DevState&, const double*, long long*,    \
-                                                cudaStream_t);
+                                                cudaStream_t);                                                   \
+    extern template bool coop_step_fits_t<NF>(const DevParams&, long long);                                      \
+    extern template cudaError_t launch_rk4_step_coop_t<NF>(const DevParams&, const DevState&, double* const*,    \
+                                                           long long, StepCtl*, int, cudaStream_t);
 EMU_EXTERN(2)
 EMU_EXTERN(3)
 
@@ -102,6 +105,18 @@ void launch_rk4_stage(int nf, const DevParams& P, const DevState& S, int s, cons
 {
     if (nf == 2) launch_rk4_stage_t<2>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt_mode, st);
     else launch_rk4_stage_t<3>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt_mode, st);
+}
+
+bool coop_step_fits(int nf, const DevParams& P, long long n)
+{
+    return nf == 2 ? coop_step_fits_t<2>(P, n) : coop_step_fits_t<3>(P, n);
+}
+
+cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, double* const mesh[4], long long nmesh,
+                                 StepCtl* ctl, int dt_mode, cudaStream_t st)
+{
+    return nf == 2 ? launch_rk4_step_coop_t<2>(P, S, mesh, nmesh, ctl, dt_mode, st)
+                   : launch_rk4_step_coop_t<3>(P, S, mesh, nmesh, ctl, dt_mode, st);
 }
 
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,

@@ -57,6 +57,7 @@ struct StepCtl {
     int last;            // the step in progress is the final one (clipped to end_time)
     unsigned int blocks_done;
     unsigned long long vmax_bits[2];   // max V_adaptive, V_stupid (non-negative doubles as bits)
+    unsigned int bar_count, bar_gen;   // grid barrier of the cooperative step kernel
 };
 
 enum DtMode : int { DT_QUERY = 0, DT_INIT = 1, DT_ADVANCE = 2 };
@@ -84,6 +85,11 @@ void launch_combine(int nf, const DevParams& P, const DevState& S, const double*
 void launch_rk4_stage(int nf, const DevParams& P, const DevState& S, int s, const double* mesh_in,
                       double* mesh_out, double* mesh_zero, long long nzero, StepCtl* ctl, int dt_mode,
                       cudaStream_t st);
+// whole FP64 RK4 step in one cooperative launch; returns false (nothing
+// launched) when the grid cannot be co-resident
+bool coop_step_fits(int nf, const DevParams& P, long long n);
+cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, double* const mesh[4], long long nmesh,
+                                 StepCtl* ctl, int dt_mode, cudaStream_t st);
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
                             long long* qmesh_out, const long long* qmesh_dt, StepCtl* ctl, int dt_mode,
                             cudaStream_t st);

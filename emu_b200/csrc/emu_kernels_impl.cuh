@@ -327,18 +327,15 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
 // ===========================================================================
 // fused FP64 RK4 stage
 // ===========================================================================
-template <int NF, int WX, int WY, int WZ>
-__global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S, int s, const double* __restrict__ mesh_in,
-                                                      double* __restrict__ mesh_out, double* mesh_zero, long long nzero,
-                                                      StepCtl* ctl, int dt_mode)
+template <int NF, class SWt>
+__device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevState& S, int s,
+                                               const double* __restrict__ mesh_in, double* __restrict__ mesh_out,
+                                               double* mesh_zero, long long nzero, StepCtl* ctl, double dt)
 {
-    using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
-    if (ctl->done) return;
     zero_slice(mesh_zero, nzero);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
-    const double dt = ctl->dt;
     const long long cap = S.cap;
 
     Stencil<double> st{};
@@ -410,9 +407,71 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S
     }
     tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
                                         [](double a, int) -> double { return a; });
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S, int s, const double* __restrict__ mesh_in,
+                                                      double* __restrict__ mesh_out, double* mesh_zero, long long nzero,
+                                                      StepCtl* ctl, int dt_mode)
+{
+    if (ctl->done) return;
+    rk4_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, ctl->dt);
     // stage 4 of the device-resident loop: compute_dt on the stage-4 mesh
     // (main.cpp:193-198), which this kernel only reads
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+}
+
+// Grid-wide barrier of the cooperative step kernel (its CTAs are co-resident
+// by cooperative launch).  The wait is bounded: after kBarrierSpins polls the
+// CTA records ST_TIMEOUT in the step status and continues, so a failure can
+// never hang the GPU.
+constexpr long long kBarrierSpins = 1ll << 22;
+
+__device__ __forceinline__ void grid_barrier(StepCtl* ctl)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* genp = &ctl->bar_gen;
+        const unsigned g = *genp;
+        __threadfence();
+        if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
+            ctl->bar_count = 0u;
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            long long it = 0;
+            while (*genp == g) {
+                if (++it > kBarrierSpins) {
+                    atomicOr(&ctl->status, ST_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// Whole RK4 step in one cooperative launch (small problems whose grid fits
+// on the GPU at once): the four stage bodies separated by grid barriers, then
+// compute_dt on the stage-4 mesh.  Saves three kernel boundaries per step.
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock, 4) k_rk4_step_coop(DevParams P, DevState S, double* m0, double* m1,
+                                                            double* m2, double* m3, long long nmesh, StepCtl* ctl,
+                                                            int dt_mode)
+{
+    using SWt = SW<WX, WY, WZ>;
+    if (ctl->done) return;
+    const double dt = ctl->dt;
+    rk4_stage_body<NF, SWt>(P, S, 1, m0, m1, m2, nmesh, ctl, dt);
+    grid_barrier(ctl);
+    rk4_stage_body<NF, SWt>(P, S, 2, m1, m2, m3, nmesh, ctl, dt);
+    grid_barrier(ctl);
+    rk4_stage_body<NF, SWt>(P, S, 3, m2, m3, m0, nmesh, ctl, dt);
+    grid_barrier(ctl);
+    rk4_stage_body<NF, SWt>(P, S, 4, m3, m0, m1, nmesh, ctl, dt);
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, m3, ctl, DT_ADVANCE, reduce_blocks(P));
 }
 
 // ===========================================================================
@@ -893,6 +952,8 @@ __global__ void k_ctl_set(StepCtl* ctl, double dt, double t, double end_time, in
     ctl->last = 0;
     ctl->blocks_done = 0u;
     ctl->vmax_bits[0] = ctl->vmax_bits[1] = 0ull;
+    ctl->bar_count = 0u;
+    ctl->bar_gen = 0u;
     if (reset_status) {
         ctl->status = 0;
         ctl->bad = LLONG_MAX;
@@ -946,6 +1007,45 @@ void launch_rk4_stage_t(const DevParams& P, const DevState& S, int s, const doub
         k_rk4_stage<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, s, mesh_in, mesh_out, mesh_zero,
                                                                             nzero, ctl, dt_mode);
     });
+}
+
+template <int NF>
+bool coop_step_fits_t(const DevParams& P, long long n)
+{
+    bool ok = false;
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        auto kern = k_rk4_step_coop<NF, WXv, WYv, WZv>;
+        smem_optin(kern, bytes);
+        int per_sm = 0, dev = 0, nsm = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, bytes) == cudaSuccess)
+            ok = (long long)per_sm * nsm >= (long long)grid_for(n);
+    });
+    cudaGetLastError();
+    return ok;
+}
+
+template <int NF>
+cudaError_t launch_rk4_step_coop_t(const DevParams& P, const DevState& S, double* const mesh[4], long long nmesh,
+                                   StepCtl* ctl, int dt_mode, cudaStream_t st)
+{
+    cudaError_t err = cudaSuccess;
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        auto kern = k_rk4_step_coop<NF, WXv, WYv, WZv>;
+        smem_optin(kern, bytes);
+        DevParams Pc = P;
+        DevState Sc = S;
+        double *m0 = mesh[0], *m1 = mesh[1], *m2 = mesh[2], *m3 = mesh[3];
+        long long nm = nmesh;
+        StepCtl* c = ctl;
+        int mode = dt_mode;
+        void* args[] = {&Pc, &Sc, &m0, &m1, &m2, &m3, &nm, &c, &mode};
+        err = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid_for(S.n)), dim3(kBlock), args, bytes, st);
+    });
+    return err;
 }
 
 template <int NF>

@@ -44,6 +44,7 @@ extern "C" {
 #define EMU_ERR_PARSE    256   /* inputs file */
 #define EMU_ERR_NOMEM    512   /* allocation failed */
 #define EMU_ERR_LIMIT    1024  /* size beyond a documented limit */
+#define EMU_ERR_TIMEOUT  2048  /* a bounded device-side wait gave up (results of that step are invalid) */
 
 /* arithmetic of the path */
 #define EMU_PREC_FP64    0     /* FP64 throughout (the reference's PRECISION=DOUBLE) */
@@ -102,7 +103,9 @@ typedef struct emu_params {
     uint64_t seed;           /* counter-based RNG seed for sim types 4 and 5
                                 (the reference seeds from the clock, main.cpp:240) */
     int resort_interval;     /* steps between on-device cell re-sorts (0 = never) */
-    int fused;               /* 1: fused one-kernel-per-stage RK4 (default), 0: unfused stages */
+    int fused;               /* RK4 kernels: 2 (default) one cooperative launch per step when
+                                the grid fits on the GPU at once (FP64), else as 1;
+                                1: one fused kernel per stage; 0: unfused stages */
 } emu_params;
 
 /* summary of a device-resident run (emu_evolve) */

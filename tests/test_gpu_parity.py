@@ -40,16 +40,17 @@ def test_deposit_rhs_dt_vs_golden(path):
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=golden_ids())
-@pytest.mark.parametrize("integ", ["rk4_fused", "rk4_unfused", "fe", "trapezoid", "ssprk3"])
+@pytest.mark.parametrize("integ", ["rk4_coop", "rk4_fused", "rk4_unfused", "fe", "trapezoid", "ssprk3"])
 def test_one_step_vs_golden(path, integ):
     p, d = load_golden(path)
     nc = 3 + 8 * p.nflavors ** 2
-    kw = {"rk4_fused": dict(integration_type=1, rk_type=4, fused=1),
+    kw = {"rk4_coop": dict(integration_type=1, rk_type=4, fused=2),
+          "rk4_fused": dict(integration_type=1, rk_type=4, fused=1),
           "rk4_unfused": dict(integration_type=1, rk_type=4, fused=0),
           "fe": dict(integration_type=0, rk_type=4, fused=0),
           "trapezoid": dict(integration_type=1, rk_type=2, fused=0),
           "ssprk3": dict(integration_type=1, rk_type=3, fused=0)}[integ]
-    k = {"rk4_fused": 4, "rk4_unfused": 4, "fe": 0, "trapezoid": 2, "ssprk3": 3}[integ]
+    k = {"rk4_coop": 4, "rk4_fused": 4, "rk4_unfused": 4, "fe": 0, "trapezoid": 2, "ssprk3": 3}[integ]
     with _ctx(p, resort_interval=0, **kw) as c:
         c.load_particles(d["parts"])
         code, bad = c.step(float(d["dt0"]))
@@ -76,10 +77,11 @@ def _c2_small(ncz=16, ndirs=20, **kw):
     return p
 
 
-@pytest.mark.parametrize("resort", [0, 1, 3])
-def test_evolve_matches_oracle(resort):
-    """device-resident loop (CUDA graph, device dt) vs the oracle's evolve"""
-    p = _c2_small(resort_interval=resort)
+@pytest.mark.parametrize("resort,fused", [(0, 2), (1, 2), (3, 2), (0, 1), (3, 1)])
+def test_evolve_matches_oracle(resort, fused):
+    """device-resident loop (cooperative step kernel or CUDA graph of stage
+    kernels, device dt) vs the oracle's evolve"""
+    p = _c2_small(resort_interval=resort, fused=fused)
     parts = api.init_particles(p)
     o = Oracle(p)
     ref, t_ref, dts, st = o.evolve(parts, 12)
