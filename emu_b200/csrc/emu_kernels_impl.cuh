@@ -333,6 +333,9 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
                                                double* mesh_zero, long long nzero, StepCtl* ctl, double dt)
 {
     constexpr int NH = NF * NF, NS = 2 * NH;
+    // whole-state preload where it fits the register budget (two flavors,
+    // one-dimensional stencil)
+    constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
     zero_slice(mesh_zero, nzero);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
@@ -346,39 +349,76 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
         vx = S.vhat[0][p];
         vy = S.vhat[1][p];
         vz = S.vhat[2][p];
+        // the stage's per-particle loads are issued together (one memory
+        // round trip); the state arrays never alias
+        const double* __restrict__ fin = s == 1 ? S.f0 : S.fs;
+        const double* __restrict__ f0p = S.f0;
+        const double* __restrict__ accp = S.acc;
+        const double vsc = S.vscale[p];
+        const double Nsp[2] = {S.Nn[0][p], S.Nn[1][p]};
+        const bool hoist = PRELOAD && s == 4;
+        const double Lsp[2] = {hoist ? S.Ll[0][p] : 0.0, hoist ? S.Ll[1][p] : 0.0};
+        const double t_in = hoist ? S.time[p] : 0.0;
+        constexpr int PRE = PRELOAD ? NS : 1;
+        double fc[PRE], yv[PRE], av[PRE];
+        if constexpr (PRELOAD) {
+#pragma unroll
+            for (int c = 0; c < NS; c++) fc[c] = fin[c * cap + p];
+            if (s > 1) {
+#pragma unroll
+                for (int c = 0; c < NS; c++) {
+                    yv[c] = f0p[c * cap + p];
+                    av[c] = accp[c * cap + p];
+                }
+            }
+        }
         double V[NS];
         make_stencil<double>(P, x, y, z, st);
-        potential_fp64<NF, SWt>(P, mesh_in, st, vx, vy, vz, S.vscale[p], V);
+        potential_fp64<NF, SWt>(P, mesh_in, st, vx, vy, vz, vsc, V);
         const double bw = dt * kRK4B[s - 1];
         const double aw = s < 4 ? dt * kRK4A[s] : 0.0;
         int stt = 0;
         // one species at a time keeps the live state small
 #pragma unroll
         for (int sp = 0; sp < 2; sp++) {
-            double f[NH], K[NH];
+            double fl[NH], K[NH];
+            double* f = fl;
+            if constexpr (PRELOAD) f = fc + sp * NH;
+            else {
 #pragma unroll
-            for (int e = 0; e < NH; e++) f[e] = (s == 1 ? S.f0 : S.fs)[(sp * NH + e) * cap + p];
+                for (int e = 0; e < NH; e++) fl[e] = fin[(sp * NH + e) * cap + p];
+            }
             commutator<NF, double>(V + sp * NH, f, K, P.inv_hbar);
             double* fn = f;   // reuse as the next state
             if (s < 4) {
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
                     const long long o = (sp * NH + e) * cap + p;
-                    const double y0 = (s == 1) ? f[e] : S.f0[o];
-                    const double a0 = (s == 1) ? y0 : S.acc[o];
+                    double y0, a0;
+                    if constexpr (PRELOAD) {
+                        y0 = (s == 1) ? f[e] : yv[sp * NH + e];
+                        a0 = (s == 1) ? y0 : av[sp * NH + e];
+                    } else {
+                        y0 = (s == 1) ? f[e] : f0p[o];
+                        a0 = (s == 1) ? y0 : accp[o];
+                    }
                     S.acc[o] = __dadd_rn(__dmul_rn(bw, K[e]), a0);
                     fn[e] = __dadd_rn(__dmul_rn(aw, K[e]), y0);
                     S.fs[o] = fn[e];
                 }
             } else {
 #pragma unroll
-                for (int e = 0; e < NH; e++)
-                    fn[e] = __dadd_rn(__dmul_rn(bw, K[e]), S.acc[(sp * NH + e) * cap + p]);
-                stt |= renormalize<NF>(fn, S.Ll[sp][p], P.maxError);
+                for (int e = 0; e < NH; e++) {
+                    double a0;
+                    if constexpr (PRELOAD) a0 = av[sp * NH + e];
+                    else a0 = accp[(sp * NH + e) * cap + p];
+                    fn[e] = __dadd_rn(__dmul_rn(bw, K[e]), a0);
+                }
+                stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : S.Ll[sp][p], P.maxError);
 #pragma unroll
                 for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
             }
-            const double Ns = S.Nn[sp][p];
+            const double Ns = Nsp[sp];
 #pragma unroll
             for (int e = 0; e < NH; e++) fN[sp * NH + e] = fn[e] * Ns;
         }
@@ -387,7 +427,7 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
             // stage: x += (dt*b_i) * (pup/pupt*c), time += (dt*b_i) * 1
             double xn[3] = {x, y, z};
             const double kxv[3] = {vx * kC, vy * kC, vz * kC};
-            double tn = S.time[p];
+            double tn = PRELOAD ? t_in : S.time[p];
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const double w = dt * kRK4B[i];
@@ -414,8 +454,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S
                                                       double* __restrict__ mesh_out, double* mesh_zero, long long nzero,
                                                       StepCtl* ctl, int dt_mode)
 {
-    if (ctl->done) return;
-    rk4_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, ctl->dt);
+    const int done = ctl->done;
+    const double dt = ctl->dt;   // both control loads in one round trip
+    if (done) return;
+    rk4_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt);
     // stage 4 of the device-resident loop: compute_dt on the stage-4 mesh
     // (main.cpp:193-198), which this kernel only reads
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
@@ -462,8 +504,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_step_coop(DevParams P, DevSta
                                                             int dt_mode)
 {
     using SWt = SW<WX, WY, WZ>;
-    if (ctl->done) return;
+    const int done = ctl->done;
     const double dt = ctl->dt;
+    if (done) return;
     rk4_stage_body<NF, SWt>(P, S, 1, m0, m1, m2, nmesh, ctl, dt);
     grid_barrier(ctl);
     rk4_stage_body<NF, SWt>(P, S, 2, m1, m2, m3, nmesh, ctl, dt);
@@ -688,10 +731,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
     using H = Herm<NF>;
     using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
-    if (ctl->done) return;
+    constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
+    const int done = ctl->done;
+    const double dt = ctl->dt;   // both control loads in one round trip
+    if (done) return;
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
-    const double dt = ctl->dt;
     const long long cap = S.cap;
 
     Stencil<float> st{};
@@ -702,6 +747,30 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
         vx = S.vhat32[0][p];
         vy = S.vhat32[1][p];
         vz = S.vhat32[2][p];
+        // the stage's per-particle loads are issued together (one memory
+        // round trip; all of the state for two flavors in 1D, the
+        // per-species scalars otherwise); the state arrays never alias
+        const double* __restrict__ f0p = S.f0;
+        const float* __restrict__ k32p = S.k32;
+        const float* __restrict__ ks32p = S.ksum32;
+        const double vs = S.vscale[p];
+        const float Nsp[2] = {S.N32[0][p], S.N32[1][p]};
+        const bool hoist = PRELOAD && s == 4;
+        const double Lsp[2] = {hoist ? S.Ll[0][p] : 0.0, hoist ? S.Ll[1][p] : 0.0};
+        const double t_in = hoist ? S.time[p] : 0.0;
+        const double pu[4] = {hoist ? S.pup[0][p] : 0.0, hoist ? S.pup[1][p] : 0.0, hoist ? S.pup[2][p] : 0.0,
+                              hoist ? S.pup[3][p] : 1.0};
+        constexpr int PRE = PRELOAD ? NS : 1;
+        double y0a[PRE];
+        float ka[PRE], ksa[PRE];
+        if constexpr (PRELOAD) {
+#pragma unroll
+            for (int c = 0; c < NS; c++) {
+                y0a[c] = f0p[c * cap + p];
+                ka[c] = s > 1 ? k32p[c * cap + p] : 0.f;
+                ksa[c] = s > 1 ? ks32p[c * cap + p] : 0.f;
+            }
+        }
         make_stencil<float>(P, x, y, z, st);
         // FP32 self-interaction part, trace removed (it commutes)
         float hs[NH];
@@ -714,7 +783,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
         for (int e = 0; e < NH; e++)
             if (H::is_diag(e)) hs[e] -= tr;
         const float ih = (float)P.inv_hbar;
-        const double vs = S.vscale[p];
         const double mat = P.sqrt2GF_inv_vol * P.matter;
         const double aw = s > 1 ? dt * kRK4A[s - 1] : 0.0;
         const double an = s < 4 ? dt * kRK4A[s] : 0.0;
@@ -727,8 +795,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
 #pragma unroll
             for (int e = 0; e < NH; e++) {
                 const long long o = (sp * NH + e) * cap + p;
-                y0[e] = S.f0[o];
-                f[e] = s > 1 ? y0[e] + aw * (double)S.k32[o] : y0[e];
+                float k;
+                if constexpr (PRELOAD) {
+                    y0[e] = y0a[sp * NH + e];
+                    k = ka[sp * NH + e];
+                } else {
+                    y0[e] = f0p[o];
+                    k = s > 1 ? k32p[o] : 0.f;
+                }
+                f[e] = s > 1 ? y0[e] + aw * (double)k : y0[e];
             }
             // nubar: H_SI conjugated and negated (generate_code.py:317-355)
             float hsn[NH], f32[NH], ksi[NH];
@@ -750,29 +825,37 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
                 for (int e = 0; e < NH; e++) {
                     const long long o = (sp * NH + e) * cap + p;
                     const float kc = (float)(Kv[e] + (double)ksi[e]);
+                    float ks;
+                    if constexpr (PRELOAD) ks = ksa[sp * NH + e];
+                    else ks = s > 1 ? ks32p[o] : 0.f;
                     S.k32[o] = kc;
-                    S.ksum32[o] = (s == 1) ? kc : fmaf(2.f, kc, S.ksum32[o]);
+                    S.ksum32[o] = (s == 1) ? kc : fmaf(2.f, kc, ks);
                     fn[e] = y0[e] + an * (double)kc;
                 }
             } else {
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
                     const long long o = (sp * NH + e) * cap + p;
-                    fn[e] = y0[e] + w6 * ((double)S.ksum32[o] + (Kv[e] + (double)ksi[e]));
+                    float ks;
+                    if constexpr (PRELOAD) ks = ksa[sp * NH + e];
+                    else ks = ks32p[o];
+                    fn[e] = y0[e] + w6 * ((double)ks + (Kv[e] + (double)ksi[e]));
                 }
-                stt |= renormalize<NF>(fn, S.Ll[sp][p], P.maxError);
+                stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : S.Ll[sp][p], P.maxError);
 #pragma unroll
                 for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
             }
-            const float Ns = S.N32[sp][p];
+            const float Ns = Nsp[sp];
 #pragma unroll
             for (int e = 0; e < NH; e++) fN[sp * NH + e] = (float)fn[e] * Ns;
         }
         if (s == 4) {
             double xn[3] = {x, y, z};
-            double tn = S.time[p];
-            const double ipt = 1.0 / S.pup[3][p];
-            const double kxv[3] = {S.pup[0][p] * ipt * kC, S.pup[1][p] * ipt * kC, S.pup[2][p] * ipt * kC};
+            double tn = PRELOAD ? t_in : S.time[p];
+            const double pq[4] = {PRELOAD ? pu[0] : S.pup[0][p], PRELOAD ? pu[1] : S.pup[1][p],
+                                  PRELOAD ? pu[2] : S.pup[2][p], PRELOAD ? pu[3] : S.pup[3][p]};
+            const double ipt = 1.0 / pq[3];
+            const double kxv[3] = {pq[0] * ipt * kC, pq[1] * ipt * kC, pq[2] * ipt * kC};
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const double w = dt * kRK4B[i];
