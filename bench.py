@@ -39,7 +39,7 @@ from emu_b200 import workloads as W  # noqa: E402
 METRIC = "particle RK4 steps/s on 1 B200: mixed vs FP64 at stated err; % of HBM peak"
 
 
-def workload(name, precision, cells=None, fused=None):
+def workload(name, precision, cells=None, fused=None, resort=None):
     """cells overrides the cell count (z cells for c2/c3, cells per side for
     c5) to run a smaller case of the same workload (profiling)."""
     if name == "c2":
@@ -58,6 +58,8 @@ def workload(name, precision, cells=None, fused=None):
         p.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
     if fused:
         p.fused = fused
+    if resort is not None:
+        p.resort_interval = resort
     return p, desc
 
 
@@ -166,7 +168,7 @@ def run_reference(args):
     ws, rank, local = dist_setup(args)
     if rank != 0:
         return
-    p, desc = workload(args.workload, args.precision, args.cells, args.fused)
+    p, desc = workload(args.workload, args.precision, args.cells, args.fused, args.resort)
     recs = api.init_particles(p)
     nthreads = os.cpu_count() or 1
     from oracle.oracle import Oracle, RefHarness, have_ref
@@ -211,7 +213,7 @@ def run_emu(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    p, desc = workload(args.workload, args.precision, args.cells, args.fused)
+    p, desc = workload(args.workload, args.precision, args.cells, args.fused, args.resort)
     mixed = p.precision == api.PREC_MIXED
     nf = p.nflavors
     recs = api.init_particles(p)
@@ -360,6 +362,8 @@ def main():
     ap.add_argument("--cells", type=int, default=None, help="smaller case of the workload (cells per side)")
     ap.add_argument("--fused", type=int, default=None, choices=[1, 2],
                     help="RK4 kernels: 2 one cooperative launch per step when it fits (default), 1 per stage")
+    ap.add_argument("--resort", type=int, default=None,
+                    help="steps between on-device cell re-sorts (0 never; default the workload's)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=15.0)

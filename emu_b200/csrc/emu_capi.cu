@@ -469,6 +469,13 @@ int emu_create(const emu_params* p, emu_context** out)
     ctx->nreal = emu_nreal(ctx->nf);
     ctx->mixed = p->precision == EMU_PREC_MIXED;
     emu::make_devparams(*p, ctx->P);
+    if (ctx->prm.resort_interval < 0) {
+        // automatic: a 27-cell stencil loses its per-CTA cell runs within a
+        // step or two once particles leave their cells, a 1D stencil within
+        // several
+        const int cells = ctx->P.w[0] * ctx->P.w[1] * ctx->P.w[2];
+        ctx->prm.resort_interval = cells > 9 ? 1 : 4;
+    }
     int r = EMU_OK;
     auto bail = [&](int code) {
         g_host_err = ctx->err;

@@ -455,7 +455,7 @@ void emu_params_default(emu_params* p)
     p->direction_generator = 0;
     p->ndirections = 0;
     p->seed = 0;
-    p->resort_interval = 8;
+    p->resort_interval = -1;
     p->fused = 2;
 }
 
@@ -498,7 +498,7 @@ int emu_parse_inputs(const char* path, int n_overrides, const char* const* overr
     p.direction_generator = g.i_or("emu.direction_generator", 0);
     p.ndirections = g.i_or("emu.ndirections", 0);
     p.seed = (uint64_t)g.d_or("emu.seed", 0);
-    p.resort_interval = g.i_or("emu.resort_interval", 8);
+    p.resort_interval = g.i_or("emu.resort_interval", -1);
     p.fused = g.i_or("emu.fused", 2);
     // integrator keys read by the AMReX TimeIntegrator
     p.integration_type = g.i("integration.type");

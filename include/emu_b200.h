@@ -102,7 +102,9 @@ typedef struct emu_params {
     int ndirections;
     uint64_t seed;           /* counter-based RNG seed for sim types 4 and 5
                                 (the reference seeds from the clock, main.cpp:240) */
-    int resort_interval;     /* steps between on-device cell re-sorts (0 = never) */
+    int resort_interval;     /* steps between on-device cell re-sorts (0 = never,
+                                < 0 = automatic: every step for 3D stencils,
+                                every 4 steps otherwise; default -1) */
     int fused;               /* RK4 kernels: 2 (default) one cooperative launch per step when
                                 the grid fits on the GPU at once (FP64), else as 1;
                                 1: one fused kernel per stage; 0: unfused stages */
