@@ -130,6 +130,10 @@ SIGNATURES = {
     "emu_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "emu_deposit_noalloc": (ctypes.c_int, [_P(EmuParams), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "emu_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D,
+                                           _P(EmuRunInfo)]),
+    "emu_adjoint_objective": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
+    "emu_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D]),
 }
 
 
@@ -340,6 +344,37 @@ class Context:
         if code & ~(EMU_ERR_TRACE | EMU_ERR_NEGDIAG | EMU_ERR_LENGTH | EMU_ERR_DT):
             self._ck(code, "emu_evolve")
         return info
+
+    # ---- discrete adjoint (FP64 RK4) ----
+    def adjoint_forward(self, nsteps, checkpoint_interval, start_time=0.0):
+        """Recorded run of nsteps from the loaded state; returns (dts, info)."""
+        dts = np.zeros(int(nsteps))
+        info = EmuRunInfo()
+        self._ck(self.lib.emu_adjoint_forward(self.h, int(nsteps), int(checkpoint_interval), float(start_time),
+                                              _dptr(dts), ctypes.byref(info)), "emu_adjoint_forward")
+        return dts, info
+
+    def adjoint_objective(self, gradient=True):
+        """(J, dJ/df [n, 2nf^2], dJ/d(N, Nbar) [n, 2]) of the current state, load order."""
+        n = self.num_particles()
+        J = np.zeros(1)
+        lf = np.zeros((n, 2 * self.nf * self.nf)) if gradient else None
+        lN = np.zeros((n, 2)) if gradient else None
+        null = ctypes.cast(None, _D)
+        self._ck(self.lib.emu_adjoint_objective(self.h, _dptr(J), _dptr(lf) if gradient else null,
+                                                _dptr(lN) if gradient else null), "emu_adjoint_objective")
+        return float(J[0]), lf, lN
+
+    def adjoint_backward(self, lam_f_final, lam_N_final=None):
+        """(dJ/df0 [n, 2nf^2], dJ/d(N, Nbar) [n, 2]) of the recorded run's initial state."""
+        n = self.num_particles()
+        lf = np.ascontiguousarray(lam_f_final, dtype=np.float64).reshape(n, 2 * self.nf * self.nf)
+        lN = None if lam_N_final is None else np.ascontiguousarray(lam_N_final, dtype=np.float64).reshape(n, 2)
+        out_f = np.zeros_like(lf)
+        out_N = np.zeros((n, 2))
+        self._ck(self.lib.emu_adjoint_backward(self.h, _dptr(lf), ctypes.cast(None, _D) if lN is None else _dptr(lN),
+                                               _dptr(out_f), _dptr(out_N)), "emu_adjoint_backward")
+        return out_f, out_N
 
     def evolve_begin(self, start_time, end_time, max_steps):
         self._ck(self.lib.emu_evolve_begin(self.h, float(start_time), float(end_time), int(max_steps)),

@@ -22,9 +22,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
 
-SOURCES = ["emu_k_fp64_3.cu", "emu_k_mixed_3.cu", "emu_k_fp64_2.cu", "emu_k_mixed_2.cu", "emu_k_misc.cu",
-           "emu_capi.cu", "emu_noalloc.cu", "emu_host.cpp", "emu_init.cpp"]
-HEADERS = ["emu_device.cuh", "emu_kernels.cuh", "emu_kernels_impl.cuh", "emu_host.h"]
+SOURCES = ["emu_k_fp64_3.cu", "emu_k_mixed_3.cu", "emu_adjoint.cu", "emu_k_fp64_2.cu", "emu_k_mixed_2.cu",
+           "emu_k_misc.cu", "emu_capi.cu", "emu_noalloc.cu", "emu_host.cpp", "emu_init.cpp"]
+HEADERS = ["emu_device.cuh", "emu_kernels.cuh", "emu_kernels_impl.cuh", "emu_context.cuh", "emu_host.h"]
 
 
 def _stale(out, deps):

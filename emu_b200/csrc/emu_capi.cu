@@ -1,9 +1,7 @@
 // emu_capi.cu -- the C ABI (include/emu_b200.h): device context, particle
 // upload/download with on-device cell sorting, the step drivers (fused RK4,
 // unfused Butcher tableau, mixed precision) and the CUDA-graph step loop.
-#include "emu_b200.h"
-#include "emu_host.h"
-#include "emu_kernels.cuh"
+#include "emu_context.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -15,71 +13,29 @@
 #include <string>
 #include <vector>
 
-using emu::DevParams;
-using emu::DevState;
-using emu::StepCtl;
-
-struct emu_context {
-    emu_params prm;
-    DevParams P;
-    int nf = 2, NH = 4, NS = 8, ND = 32, nreal = 23;
-    bool mixed = false;
-    cudaStream_t stream = nullptr;      // where work is launched
-    cudaStream_t own = nullptr;         // the context's own stream
-    cudaStream_t cap_stream = nullptr;  // private stream used for graph capture
-    DevState S[2];                      // persistent particle arrays, double-buffered for re-sorts
-    int cur = 0;                        // which of S[] is current
-    void* pblock[2] = {nullptr, nullptr};
-    void* tblock = nullptr;             // transient per-step arrays
-    long long cap = 0;
-    double* mesh[4] = {nullptr, nullptr, nullptr, nullptr};
-    long long* qmesh[2] = {nullptr, nullptr};
-    float* gmesh = nullptr;
-    double* fmesh_tmp = nullptr;        // FP64 cell-major copy (mixed API calls)
-    double* planes = nullptr;           // ncomp x ncells output staging
-    StepCtl* ctl = nullptr;
-    StepCtl* ctl_host = nullptr;        // pinned
-    double* aos = nullptr;              // AoS staging (n x nreal)
-    long long aos_cap = 0;
-    unsigned *keys = nullptr, *keys2 = nullptr, *idx = nullptr, *idx2 = nullptr;
-    void* sort_tmp = nullptr;
-    size_t sort_tmp_bytes = 0;
-    int cur_mesh = 0;
-    bool fused_ready = false;
-    bool loaded = false;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int steps_since_sort = 0;
-    bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
-    std::string err;
-};
-
 namespace {
 
 thread_local std::string g_host_err;
 
-int fail(emu_context* c, int code, const std::string& msg)
+int widths(int ord) { return ord >= 2 ? 3 : (ord == 1 ? 2 : 1); }
+
+}  // namespace
+
+int emu_ctx::fail(emu_context* c, int code, const std::string& msg)
 {
     if (c) c->err = msg; else g_host_err = msg;
     return code;
 }
 
-#define CU(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess)                                                                     \
-            return fail(ctx, EMU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
-    } while (0)
-
-int check_launch(emu_context* ctx, const char* what)
+int emu_ctx::check_launch(emu_context* ctx, const char* what)
 {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     return EMU_OK;
 }
 
-int widths(int ord) { return ord >= 2 ? 3 : (ord == 1 ? 2 : 1); }
-
-}  // namespace
+using emu_ctx::check_launch;
+using emu_ctx::fail;
 
 void emu_host::set_error(const std::string& msg) { g_host_err = msg; }
 
@@ -395,6 +351,7 @@ int resort(emu_context* ctx)
     if ((r = check_launch(ctx, "resort"))) return r;
     ctx->cur = 1 - ctx->cur;
     ctx->steps_since_sort = 0;
+    ctx->adj_valid = false;   // slot order changed
     // the deposited meshes are order independent; stage 1 of the next step
     // reads the same mesh as before the re-sort
     return EMU_OK;
@@ -432,6 +389,22 @@ bool rk4_fused(const emu_context* ctx)
 }  // namespace
 
 // ===========================================================================
+int emu_ctx::step_device(emu_context* ctx)
+{
+    int r;
+    if (ctx->coop) {
+        double* const m[4] = {ctx->mesh[0], ctx->mesh[1], ctx->mesh[2], ctx->mesh[3]};
+        cudaError_t e = emu::launch_rk4_step_coop(ctx->nf, ctx->P, ctx->S[ctx->cur], m, mesh_elems(ctx), ctx->ctl,
+                                                  emu::DT_ADVANCE, ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
+    } else {
+        if (!ctx->graph[ctx->cur] && (r = build_graph(ctx))) return r;
+        CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+    }
+    ctx->cur_mesh = ctx->mixed ? 1 : 3;
+    return EMU_OK;
+}
+
 extern "C" {
 
 int emu_abi_version(void) { return EMU_B200_ABI_VERSION; }
@@ -537,6 +510,7 @@ void emu_destroy(emu_context* ctx)
     if (ctx->aos) cudaFree(ctx->aos);
     if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
     if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
+    emu_ctx::adjoint_free(ctx);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     delete ctx;
@@ -590,6 +564,7 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     // fused == 2 (default): one cooperative launch per step when the grid fits
     ctx->coop = !ctx->mixed && ctx->prm.fused == 2 && rk4_fused(ctx) && emu::coop_step_fits(ctx->nf, ctx->P, n);
     ctx->loaded = true;
+    ctx->adj_valid = false;
     ctx->steps_since_sort = 0;
     if ((r = deposit_current(ctx))) return r;
     CU(cudaStreamSynchronize(ctx->stream));
@@ -753,17 +728,7 @@ int emu_evolve_steps(emu_context* ctx, int nsteps)
     if (!ctx) return EMU_ERR_ARG;
     int r;
     for (int i = 0; i < nsteps; i++) {
-        if (ctx->coop) {
-            double* const m[4] = {ctx->mesh[0], ctx->mesh[1], ctx->mesh[2], ctx->mesh[3]};
-            cudaError_t e = emu::launch_rk4_step_coop(ctx->nf, ctx->P, ctx->S[ctx->cur], m, mesh_elems(ctx),
-                                                      ctx->ctl, emu::DT_ADVANCE, ctx->stream);
-            if (e != cudaSuccess)
-                return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
-        } else {
-            if (!ctx->graph[ctx->cur] && (r = build_graph(ctx))) return r;
-            CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
-        }
-        ctx->cur_mesh = ctx->mixed ? 1 : 3;
+        if ((r = emu_ctx::step_device(ctx))) return r;
         if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
             if ((r = resort(ctx))) return r;
     }

@@ -1,0 +1,72 @@
+// emu_context.cuh -- the device context behind the C ABI handle, shared by
+// the translation units that implement the C ABI (emu_capi.cu: particles,
+// steps, output; emu_adjoint.cu: the discrete adjoint).
+#pragma once
+#include "emu_b200.h"
+#include "emu_host.h"
+#include "emu_kernels.cuh"
+
+#include <string>
+
+using emu::DevParams;
+using emu::DevState;
+using emu::StepCtl;
+
+struct emu_adjoint;   // adjoint checkpoints and work arrays (emu_adjoint.cu)
+
+struct emu_context {
+    emu_params prm;
+    DevParams P;
+    int nf = 2, NH = 4, NS = 8, ND = 32, nreal = 23;
+    bool mixed = false;
+    cudaStream_t stream = nullptr;      // where work is launched
+    cudaStream_t own = nullptr;         // the context's own stream
+    cudaStream_t cap_stream = nullptr;  // private stream used for graph capture
+    DevState S[2];                      // persistent particle arrays, double-buffered for re-sorts
+    int cur = 0;                        // which of S[] is current
+    void* pblock[2] = {nullptr, nullptr};
+    void* tblock = nullptr;             // transient per-step arrays
+    long long cap = 0;
+    double* mesh[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long* qmesh[2] = {nullptr, nullptr};
+    float* gmesh = nullptr;
+    double* fmesh_tmp = nullptr;        // FP64 cell-major copy (mixed API calls)
+    double* planes = nullptr;           // ncomp x ncells output staging
+    StepCtl* ctl = nullptr;
+    StepCtl* ctl_host = nullptr;        // pinned
+    double* aos = nullptr;              // AoS staging (n x nreal)
+    long long aos_cap = 0;
+    unsigned *keys = nullptr, *keys2 = nullptr, *idx = nullptr, *idx2 = nullptr;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int cur_mesh = 0;
+    bool fused_ready = false;
+    bool loaded = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int steps_since_sort = 0;
+    bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
+    emu_adjoint* adj = nullptr;         // allocated by the first adjoint call
+    bool adj_valid = false;             // a recorded run matches the slot order
+    std::string err;
+};
+
+namespace emu_ctx {
+
+// record msg on the context (or the thread's host error when c is null)
+int fail(emu_context* c, int code, const std::string& msg);
+// EMU_ERR_CUDA with what + the pending launch error, if any
+int check_launch(emu_context* ctx, const char* what);
+// one device-resident step of the fused RK4 loop (cooperative kernel or
+// graph), without the periodic re-sort; dt comes from the device control
+int step_device(emu_context* ctx);
+// frees the adjoint arrays (emu_destroy)
+void adjoint_free(emu_context* ctx);
+
+}  // namespace emu_ctx
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return emu_ctx::fail(ctx, EMU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)

@@ -238,6 +238,36 @@ int emu_last_error(const emu_context* ctx, char* buf, size_t len);
 int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n, double* d_mesh_out,
                         void* stream);
 
+/*
+ * Discrete adjoint of the FP64 RK4 evolution.  No counterpart in the
+ * reference (it has no derivatives).  Arrays are host memory in load order:
+ * lam_f rows hold dJ/d(the 2 nflavors^2 flavor reals of a record, nu then
+ * nubar, in the record's f order); lam_N rows hold (dJ/dN, dJ/dNbar).
+ *
+ * emu_adjoint_forward: nsteps device-resident RK4 steps from the loaded
+ * state with the configured timestep rule, recording every step's dt (into
+ * dts when not NULL) and a checkpoint of (f, x) every checkpoint_interval
+ * steps.  Particles keep their order (no re-sort) during a recorded run.
+ * Requires precision FP64, integration_type 1, rk_type 4, fused >= 1.
+ *
+ * emu_adjoint_objective: J = sum over cells |N_emu|^2 / V_cell of the
+ * current state (N_emu: the neutrino e-mu off-diagonal number deposited in
+ * a cell; J is the domain integral of |n_emu|^2) and, when the pointers are
+ * not NULL, dJ/df (n x 2nf^2) and dJ/d(N, Nbar) (n x 2) of that state.
+ *
+ * emu_adjoint_backward: given dJ/df of the final state of the recorded run
+ * (lam_f_final, n x 2nf^2) and optionally dJ/d(N, Nbar) taken at the final
+ * state (lam_N_final, n x 2, NULL = 0), the gradient with respect to the
+ * run's initial f (lam_f0) and N, Nbar (lam_N0), with the recorded dt held
+ * fixed.  Recomputes each checkpoint segment and each step's stages.  The
+ * context's particle state is unchanged.
+ */
+int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, double start_time, double* dts,
+                        emu_run_info* info);
+int emu_adjoint_objective(emu_context* ctx, double* J, double* lam_f, double* lam_N);
+int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const double* lam_N_final, double* lam_f0,
+                         double* lam_N0);
+
 #ifdef __cplusplus
 }
 #endif
