@@ -46,6 +46,10 @@ def workload(name, precision, cells=None, fused=None, resort=None):
         p = W.c2_fast_flavor_1d(ncell_z=cells or 128)
         desc = "C2 fast-flavor 1D: 2 flavors, 1x1x%d cells over %g cm, 80 Fibonacci directions/cell" % (
             p.ncell[2], p.Lz)
+    elif name == "c4":
+        p = W.c4_adjoint()
+        desc = ("C4 adjoint: C2 sizes (2 flavors, 1x1x%d cells, 80 directions/cell), %d RK4 steps, "
+                "checkpoints every 25 steps" % (p.ncell[2], p.nsteps))
     elif name == "c3":
         p = W.c3_three_flavor_1d(ncell_z=cells or 1024)
         desc = "C3 3-flavor 1D: 1x1x%d cells, 378 ring directions/cell" % p.ncell[2]
@@ -344,11 +348,54 @@ def run_emu(args):
         "wall_s": wall,
         "kernel_ms_per_step": [float(x) for x in kms.mean(axis=0)],
     }
+    if args.workload == "c4":
+        out["adjoint"] = run_adjoint(ctx, recs, p, stream, total_ms / args.steps)
     ctx.close()
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_adjoint(ctx, recs, p, stream, fwd_ms_per_step, interval=25):
+    """C4: recorded forward run (checkpoints) + J + backward sweep, device
+    time with CUDA events on the context's stream, against the plain
+    forward step time of the timed loop."""
+    import torch
+    nsteps = int(p.nsteps)
+    ctx.load_particles(recs)
+    ctx.adjoint_forward(nsteps, interval)            # warm-up (allocations)
+    J, lf, lN = ctx.adjoint_objective()
+    ctx.adjoint_backward(lf, lN)
+    # plain forward under the same conditions (back-to-back steps, no L2 flush)
+    ctx.load_particles(recs)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.evolve(nsteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / nsteps
+    ctx.load_particles(recs)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
+    ctx.adjoint_forward(nsteps, interval)
+    ev[1].record(stream)
+    J, lf, lN = ctx.adjoint_objective()
+    ev[2].record(stream)
+    g, gN = ctx.adjoint_backward(lf, lN)
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    rec_ms = ev[0].elapsed_time(ev[1])
+    bwd_ms = ev[2].elapsed_time(ev[3])
+    return {"steps": nsteps, "checkpoint_interval": interval, "J": J,
+            "record_ms_per_step": rec_ms / nsteps, "backward_ms_per_step": bwd_ms / nsteps,
+            "forward_ms_per_step": plain_ms, "forward_ms_per_step_l2_flushed": fwd_ms_per_step,
+            "backward_over_forward": bwd_ms / nsteps / plain_ms,
+            "record_plus_backward_over_forward": (rec_ms + bwd_ms) / nsteps / plain_ms,
+            "grad_max_abs": float(np.abs(g).max()),
+            "note": "record = forward run with checkpoints; backward = per segment a forward recompute "
+                    "from its checkpoint storing stage states, then the adjoint sweep (dt of each step "
+                    "held at its recorded value)"}
 
 
 def main():
@@ -357,7 +404,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="emu", choices=["emu", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"])
     ap.add_argument("--cells", type=int, default=None, help="smaller case of the workload (cells per side)")
     ap.add_argument("--fused", type=int, default=None, choices=[1, 2],

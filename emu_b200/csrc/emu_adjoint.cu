@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -47,19 +48,23 @@ struct emu_adjoint {
     int NS = 0;
     int nsteps = 0, interval = 0, nck = 0;
     bool recorded = false;
+    bool store = false;         // stage states of a whole segment fit (else one step at a time)
     double t0 = 0.0;
     std::vector<double> dts;
+    std::vector<char> resorted; // segment c began with a cell re-sort (permutation perm[c])
     double* dts_dev = nullptr;
-    double* ck = nullptr;       // nck x (NS + 3) x cap: Y_0 then x, y, z
-    double* seg = nullptr;      // interval x (NS + 3) x cap
-    double* work = nullptr;     // stage states, adjoint state, recompute state
+    double* ck = nullptr;       // nck x (NS + 3) x cap: Y_0 then x, y, z per checkpoint
+    unsigned* perm = nullptr;   // nck x cap gather permutations of the segment-start re-sorts
+    double* seg = nullptr;      // interval x (NS + 3) x cap: Y_0, x of every step of a segment
+    double* sst = nullptr;      // stored stage states (4 x NS x cap per step)
+    double* mst = nullptr;      // stored meshes M_1..M_4 per step
+    double* stat = nullptr;     // two working copies of the static particle fields
+    double* work = nullptr;
     double* lmesh[4] = {};      // adjoint meshes (rotating)
     double* nex = nullptr;      // ncells x 2 objective components
     long long seg_slots = 0, ck_slots = 0;
-    // views into work
-    double *Y[5] = {}, *Yn = nullptr, *acc = nullptr;
-    double *lamY0 = nullptr, *lamn = nullptr, *lamYd = nullptr, *lamN = nullptr;
-    double *wf = nullptr, *wpos = nullptr, *wtime = nullptr;
+    double *acc = nullptr, *lamY0 = nullptr, *lamN = nullptr, *lamn = nullptr, *lamYd = nullptr;
+    double *wf = nullptr, *lamtmp = nullptr, *wpos = nullptr, *wtime = nullptr;
     double* rows = nullptr;     // n x NS staging for host transfers
 };
 
@@ -188,14 +193,12 @@ __device__ __forceinline__ void gather_deposit_adjoint(const DevParams& P, const
 // Stage recompute: K = RHS(Yin, M_s); s < 4: acc, Y_{s+1} = Y0 + a dt K and
 // its deposit; s == 4: Y_n = acc + b4 dt K.  Same arithmetic as the forward
 // stage kernel.
-template <int NF, int WX, int WY, int WZ>
-__global__ void __launch_bounds__(kBlock) k_adj_fwd_stage(DevParams P, DevState S, int s, double dt,
-                                                          const double* __restrict__ Yin, const double* __restrict__ Y0,
-                                                          double* __restrict__ acc, double* __restrict__ Yout,
-                                                          const double* __restrict__ mesh_in,
-                                                          double* __restrict__ mesh_out)
+template <int NF, class SWt>
+__device__ __forceinline__ void adj_fwd_stage_body(const DevParams& P, const DevState& S, int s, double dt,
+                                                   const double* __restrict__ Yin, const double* __restrict__ Y0,
+                                                   double* __restrict__ acc, double* __restrict__ Yout,
+                                                   const double* __restrict__ mesh_in, double* __restrict__ mesh_out)
 {
-    using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
@@ -240,6 +243,39 @@ __global__ void __launch_bounds__(kBlock) k_adj_fwd_stage(DevParams P, DevState 
                                             [](double a, int) -> double { return a; });
 }
 
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_adj_fwd_stage(DevParams P, DevState S, int s, double dt,
+                                                          const double* __restrict__ Yin, const double* __restrict__ Y0,
+                                                          double* __restrict__ acc, double* __restrict__ Yout,
+                                                          const double* __restrict__ mesh_in,
+                                                          double* __restrict__ mesh_out)
+{
+    adj_fwd_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, dt, Yin, Y0, acc, Yout, mesh_in, mesh_out);
+}
+
+// deposit of (f N) at S.pos (k_deposit's body)
+template <int NF, class SWt>
+__device__ __forceinline__ void adj_deposit_body(const DevParams& P, const DevState& S, const double* __restrict__ f,
+                                                 double* __restrict__ mesh)
+{
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    Stencil<double> st{};
+    double fN[NS] = {};
+    double vx = 0, vy = 0, vz = 0;
+    if (active) {
+        make_stencil<double>(P, S.pos[0][p], S.pos[1][p], S.pos[2][p], st);
+        vx = S.vhat[0][p];
+        vy = S.vhat[1][p];
+        vz = S.vhat[2][p];
+#pragma unroll
+        for (int c = 0; c < NS; c++) fN[c] = f[c * S.cap + p] * S.Nn[c / NH][p];
+    }
+    tile_deposit_block<NF, SWt, double>(P, mesh, active, st, fN, vx, vy, vz,
+                                        [](double a, int) -> double { return a; });
+}
+
 struct AdjStagePtrs {
     const double* Ys;       // stage state Y_s (s >= 1)
     const double* Ynext;    // Y_{s+1} (Y_0 for s = 0), gathered stage
@@ -258,11 +294,11 @@ struct AdjStagePtrs {
 // One backward launch: (s < 4) finish stage s+1 by gathering its adjoint
 // mesh, (s >= 1) start stage s: commutator VJP and the scatter of lam_H.
 // s = 4 starts from the Renormalize VJP.
-template <int NF, int WX, int WY, int WZ>
-__global__ void __launch_bounds__(kBlock) k_adj_stage(DevParams P, DevState S, int s, double dt, AdjStagePtrs A)
+template <int NF, class SWt>
+__device__ __forceinline__ void adj_stage_body(const DevParams& P, const DevState& S, int s, double dt,
+                                               const AdjStagePtrs& A)
 {
     using H = Herm<NF>;
-    using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
     zero_slice(A.lm_zero, A.nmesh);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -339,6 +375,235 @@ __global__ void __launch_bounds__(kBlock) k_adj_stage(DevParams P, DevState S, i
     if (s >= 1)
         tile_deposit_block<NF, SWt, double>(P, A.lm_out, active, st, g, -vx, -vy, -vz,
                                             [](double a, int) -> double { return a; });
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_adj_stage(DevParams P, DevState S, int s, double dt, AdjStagePtrs A)
+{
+    adj_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, dt, A);
+}
+
+// Stage 4 of a recorded step with the step's completion: Y_n = acc + b4 dt K
+// (stored), Y_new = Renormalize(Y_n), positions advanced and wrapped, and
+// the deposit of Y_new at the new positions (the next step's M_1).  Same
+// arithmetic as the forward stage kernel.
+template <int NF, class SWt>
+__device__ __forceinline__ void adj_fwd_stage4_next_body(const DevParams& P, const DevState& S, double dt,
+                                                         const double* __restrict__ Y4, const double* __restrict__ acc,
+                                                         double* __restrict__ Yn, double* __restrict__ Ynext,
+                                                         double* __restrict__ xnext, const double* __restrict__ mesh_in,
+                                                         double* __restrict__ mesh_next)
+{
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    const long long cap = S.cap;
+    Stencil<double> st{};
+    double fN[NS] = {};
+    double vx = 0, vy = 0, vz = 0;
+    if (active) {
+        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
+        make_stencil<double>(P, x, y, z, st);
+        vx = S.vhat[0][p];
+        vy = S.vhat[1][p];
+        vz = S.vhat[2][p];
+        double V[NS];
+        potential_fp64<NF, SWt>(P, mesh_in, st, vx, vy, vz, S.vscale[p], V);
+        const double bw = dt * kRK4B[3];
+#pragma unroll
+        for (int sp = 0; sp < 2; sp++) {
+            double f[NH], K[NH];
+#pragma unroll
+            for (int e = 0; e < NH; e++) f[e] = Y4[(sp * NH + e) * cap + p];
+            commutator<NF, double>(V + sp * NH, f, K, P.inv_hbar);
+#pragma unroll
+            for (int e = 0; e < NH; e++) {
+                const long long o = (sp * NH + e) * cap + p;
+                f[e] = __dadd_rn(__dmul_rn(bw, K[e]), acc[o]);
+                Yn[o] = f[e];
+            }
+            if (Ynext) {
+                renormalize<NF>(f, S.Ll[sp][p], P.maxError);
+                const double Ns = S.Nn[sp][p];
+#pragma unroll
+                for (int e = 0; e < NH; e++) {
+                    Ynext[(sp * NH + e) * cap + p] = f[e];
+                    fN[sp * NH + e] = f[e] * Ns;
+                }
+            }
+        }
+        if (xnext) {
+            double xn[3] = {x, y, z};
+            const double kxv[3] = {vx * kC, vy * kC, vz * kC};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const double w = dt * kRK4B[i];
+#pragma unroll
+                for (int d = 0; d < 3; d++) xn[d] = __dadd_rn(__dmul_rn(w, kxv[d]), xn[d]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                xn[d] = wrap_coord(xn[d], P.L[d]);
+                xnext[d * cap + p] = xn[d];
+            }
+            make_stencil<double>(P, xn[0], xn[1], xn[2], st);
+        }
+    }
+    if (mesh_next)
+        tile_deposit_block<NF, SWt, double>(P, mesh_next, active, st, fN, vx, vy, vz,
+                                            [](double a, int) -> double { return a; });
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_adj_fwd_stage4_next(DevParams P, DevState S, double dt,
+                                                                const double* __restrict__ Y4,
+                                                                const double* __restrict__ acc, double* __restrict__ Yn,
+                                                                double* __restrict__ Ynext, double* __restrict__ xnext,
+                                                                const double* __restrict__ mesh_in,
+                                                                double* __restrict__ mesh_next)
+{
+    adj_fwd_stage4_next_body<NF, SW<WX, WY, WZ>>(P, S, dt, Y4, acc, Yn, Ynext, xnext, mesh_in, mesh_next);
+}
+
+// One checkpoint segment of len steps, stored step by step:
+//   seg  + j*seg_stride:  Y_0 (NS x cap) then x, y, z (cap each) of step j
+//   sst  + j*sst_stride:  Y_2, Y_3, Y_4, Y_n (NS x cap each)
+//   mst  + j*mst_stride:  M_1..M_4 (nmesh each)
+struct SegPtrs {
+    double* seg;
+    long long seg_stride;
+    double* sst;
+    long long sst_stride;
+    double* mst;
+    long long mst_stride;
+    const double* dts;
+    int k0, len, NS;
+    double* acc;
+    double* lm[4];
+    long long nmesh;
+    double* lamY0;
+    double* lamn;
+    double* lamYd;
+    double* lamN;
+};
+
+__host__ __device__ inline DevState seg_state(const DevState& S, const SegPtrs& G, int j)
+{
+    DevState Q = S;
+    double* base = G.seg + j * G.seg_stride + (long long)G.NS * S.cap;
+    for (int d = 0; d < 3; d++) Q.pos[d] = base + d * S.cap;
+    return Q;
+}
+
+__host__ __device__ inline double* seg_f(const SegPtrs& G, int j) { return G.seg + j * G.seg_stride; }
+
+__host__ __device__ inline double* seg_y(const SegPtrs& G, int j, int s, long long cap)
+{
+    // s = 2, 3, 4 stage states, 5 = Y_n
+    return G.sst + j * G.sst_stride + (long long)(s - 2) * G.NS * cap;
+}
+
+__host__ __device__ inline double* seg_m(const SegPtrs& G, int j, int i) { return G.mst + j * G.mst_stride + i * G.nmesh; }
+
+__host__ __device__ inline AdjStagePtrs seg_stage_ptrs(const SegPtrs& G, int j, int s, long long cap)
+{
+    const double* Y[6] = {seg_f(G, j), seg_f(G, j), seg_y(G, j, 2, cap), seg_y(G, j, 3, cap), seg_y(G, j, 4, cap),
+                          seg_y(G, j, 5, cap)};
+    AdjStagePtrs A{};
+    A.Ys = s >= 1 ? Y[s] : nullptr;
+    A.Ynext = s < 4 ? Y[s + 1] : nullptr;
+    A.Yn = Y[5];
+    A.mesh_s = s >= 1 ? seg_m(G, j, s - 1) : nullptr;
+    A.lm_in = s < 4 ? G.lm[(s + 1) % 4] : nullptr;
+    A.lm_out = s >= 1 ? G.lm[s % 4] : nullptr;
+    A.lm_zero = s >= 1 ? G.lm[(s + 3) % 4] : nullptr;
+    A.nmesh = G.nmesh;
+    A.lamY0 = G.lamY0;
+    A.lamn = G.lamn;
+    A.lamYd = G.lamYd;
+    A.lamN = G.lamN;
+    return A;
+}
+
+// Forward over a whole segment in one cooperative launch (Y_0 and x of step
+// 0 and its deposit M_1 are in place; every stored mesh starts at zero):
+// four phases per step separated by bounded grid barriers.
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, DevState S, SegPtrs G, StepCtl* ctl)
+{
+    using SWt = SW<WX, WY, WZ>;
+    const long long cap = S.cap;
+#pragma unroll 1
+    for (int j = 0; j < G.len; j++) {
+        const DevState Q = seg_state(S, G, j);
+        const double dt = G.dts[G.k0 + j];
+        const double* Y0 = seg_f(G, j);
+#pragma unroll 1
+        for (int s = 1; s <= 3; s++) {
+            adj_fwd_stage_body<NF, SWt>(P, Q, s, dt, s == 1 ? Y0 : seg_y(G, j, s, cap), Y0, G.acc,
+                                        seg_y(G, j, s + 1, cap), seg_m(G, j, s - 1), seg_m(G, j, s));
+            grid_barrier(ctl);
+        }
+        const bool more = j + 1 < G.len;
+        adj_fwd_stage4_next_body<NF, SWt>(P, Q, dt, seg_y(G, j, 4, cap), G.acc, seg_y(G, j, 5, cap),
+                                          more ? seg_f(G, j + 1) : nullptr,
+                                          more ? seg_f(G, j + 1) + (long long)G.NS * cap : nullptr, seg_m(G, j, 3),
+                                          more ? seg_m(G, j + 1, 0) : nullptr);
+        grid_barrier(ctl);
+    }
+}
+
+// Backward over a whole segment in one cooperative launch: five phases per
+// step, last step first.
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock, 4) k_adj_seg_bwd_coop(DevParams P, DevState S, SegPtrs G, StepCtl* ctl)
+{
+    using SWt = SW<WX, WY, WZ>;
+    const long long cap = S.cap;
+#pragma unroll 1
+    for (int j = G.len - 1; j >= 0; j--) {
+        const DevState Q = seg_state(S, G, j);
+        const double dt = G.dts[G.k0 + j];
+#pragma unroll 1
+        for (int s = 4; s >= 0; s--) {
+            adj_stage_body<NF, SWt>(P, Q, s, dt, seg_stage_ptrs(G, j, s, cap));
+            grid_barrier(ctl);
+        }
+    }
+}
+
+// copy (f, x) of the recompute state into a segment slot and set the
+// control dt of the step about to be recomputed
+__global__ void k_seg_save(DevState R, double* __restrict__ slot, int NS, const double* __restrict__ dts, int k,
+                           StepCtl* ctl)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0 && ctl) ctl->dt = dts[k];
+    if (p >= R.n) return;
+    const long long cap = R.cap;
+    for (int c = 0; c < NS; c++) slot[c * cap + p] = R.f0[c * cap + p];
+    for (int d = 0; d < 3; d++) slot[(NS + d) * cap + p] = R.pos[d][p];
+}
+
+// static particle fields (and the carried adjoint state) from one slot
+// order to another: dst[perm[i]] = src[i] (perm = NULL: same order)
+__global__ void k_static_scatter(DevState src, DevState dst, const unsigned* __restrict__ perm,
+                                 const double* __restrict__ lsrc, double* __restrict__ ldst, int nl)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= src.n) return;
+    const long long j = perm ? (long long)perm[i] : i;
+    const long long cap = src.cap;
+    for (int d = 0; d < 3; d++) dst.vhat[d][j] = src.vhat[d][i];
+    for (int d = 0; d < 4; d++) dst.pup[d][j] = src.pup[d][i];
+    for (int sp = 0; sp < 2; sp++) {
+        dst.Nn[sp][j] = src.Nn[sp][i];
+        dst.Ll[sp][j] = src.Ll[sp][i];
+    }
+    dst.vscale[j] = src.vscale[i];
+    dst.id[j] = src.id[i];
+    if (lsrc)
+        for (int c = 0; c < nl; c++) ldst[c * cap + j] = lsrc[c * cap + i];
 }
 
 // objective: lam_M = 2/V_cell M on the nu e-mu components, zero elsewhere;
@@ -435,6 +700,86 @@ void launch_adj_gather_t(const DevParams& P, const DevState& S, const double* lm
     EMU_W_DISPATCH(P, { k_adj_gather<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, 0, st>>>(P, S, lm, lamf, lamN); });
 }
 
+template <int NF, class K>
+bool coop_fits(K kern, int bytes, long long n)
+{
+    smem_optin(kern, bytes);
+    int per_sm = 0, dev = 0, nsm = 0;
+    const bool ok = cudaGetDevice(&dev) == cudaSuccess &&
+                    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, bytes) == cudaSuccess &&
+                    (long long)per_sm * nsm >= (long long)grid_for(n);
+    cudaGetLastError();
+    return ok;
+}
+
+template <int NF>
+bool adj_coop_fits_t(const DevParams& P, long long n)
+{
+    bool ok = false;
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        ok = coop_fits<NF>(k_adj_seg_fwd_coop<NF, WXv, WYv, WZv>, bytes, n) &&
+             coop_fits<NF>(k_adj_seg_bwd_coop<NF, WXv, WYv, WZv>, bytes, n);
+    });
+    return ok;
+}
+
+template <int NF>
+cudaError_t launch_adj_seg_coop_t(bool forward, const DevParams& P, const DevState& S, const SegPtrs& G,
+                                  StepCtl* ctl, cudaStream_t st)
+{
+    cudaError_t err = cudaSuccess;
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        smem_optin(k_adj_seg_fwd_coop<NF, WXv, WYv, WZv>, bytes);
+        smem_optin(k_adj_seg_bwd_coop<NF, WXv, WYv, WZv>, bytes);
+        const void* kern = forward ? (const void*)k_adj_seg_fwd_coop<NF, WXv, WYv, WZv>
+                                   : (const void*)k_adj_seg_bwd_coop<NF, WXv, WYv, WZv>;
+        DevParams Pc = P;
+        DevState Sc = S;
+        SegPtrs Gc = G;
+        StepCtl* c = ctl;
+        void* args[] = {&Pc, &Sc, &Gc, &c};
+        err = cudaLaunchCooperativeKernel(kern, dim3(grid_for(S.n)), dim3(kBlock), args, bytes, st);
+    });
+    return err;
+}
+
+template <int NF>
+void launch_adj_fwd_stage4_next_t(const DevParams& P, const DevState& S, double dt, const double* Y4,
+                                  const double* acc, double* Yn, double* Ynext, double* xnext, const double* mesh_in,
+                                  double* mesh_next, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+        smem_optin(k_adj_fwd_stage4_next<NF, WXv, WYv, WZv>, bytes);
+        k_adj_fwd_stage4_next<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, dt, Y4, acc, Yn, Ynext,
+                                                                                       xnext, mesh_in, mesh_next);
+    });
+}
+
+// two flavors only: the three-flavor backward body needs more than the
+// 128 registers a co-resident grid of 4 CTAs per SM allows
+bool adj_coop_fits(int nf, const DevParams& P, long long n)
+{
+    return nf == 2 && adj_coop_fits_t<2>(P, n);
+}
+
+cudaError_t launch_adj_seg_coop(int nf, bool forward, const DevParams& P, const DevState& S, const SegPtrs& G,
+                                StepCtl* ctl, cudaStream_t st)
+{
+    return nf == 2 ? launch_adj_seg_coop_t<2>(forward, P, S, G, ctl, st) : cudaErrorInvalidValue;
+}
+
+void launch_adj_fwd_stage4_next(int nf, const DevParams& P, const DevState& S, double dt, const double* Y4,
+                                const double* acc, double* Yn, double* Ynext, double* xnext, const double* mesh_in,
+                                double* mesh_next, cudaStream_t st)
+{
+    if (nf == 2) launch_adj_fwd_stage4_next_t<2>(P, S, dt, Y4, acc, Yn, Ynext, xnext, mesh_in, mesh_next, st);
+    else launch_adj_fwd_stage4_next_t<3>(P, S, dt, Y4, acc, Yn, Ynext, xnext, mesh_in, mesh_next, st);
+}
+
 void launch_adj_fwd_stage(int nf, const DevParams& P, const DevState& S, int s, double dt, const double* Yin,
                           const double* Y0, double* acc, double* Yout, const double* mesh_in, double* mesh_out,
                           cudaStream_t st)
@@ -476,15 +821,31 @@ long long mesh_elems(const emu_context* c) { return c->P.ncells * c->ND; }
 void free_adj(emu_adjoint* a)
 {
     if (!a) return;
-    if (a->dts_dev) cudaFree(a->dts_dev);
-    if (a->ck) cudaFree(a->ck);
-    if (a->seg) cudaFree(a->seg);
-    if (a->work) cudaFree(a->work);
+    for (void* p : {(void*)a->dts_dev, (void*)a->ck, (void*)a->seg, (void*)a->work, (void*)a->nex, (void*)a->rows,
+                    (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst})
+        if (p) cudaFree(p);
     for (int i = 0; i < 4; i++)
         if (a->lmesh[i]) cudaFree(a->lmesh[i]);
-    if (a->nex) cudaFree(a->nex);
-    if (a->rows) cudaFree(a->rows);
     delete a;
+}
+
+// static-field view of one of the two working blocks (12 doubles + id per slot)
+DevState stat_view(emu_adjoint* a, int w, const DevState& like)
+{
+    DevState W = like;
+    char* p = reinterpret_cast<char*>(a->stat) + (size_t)w * 13 * 8 * a->cap;
+    auto take = [&](long long count) {
+        double* r = reinterpret_cast<double*>(p);
+        p += (size_t)count * 8;
+        return r;
+    };
+    for (int d = 0; d < 3; d++) W.vhat[d] = take(a->cap);
+    for (int d = 0; d < 4; d++) W.pup[d] = take(a->cap);
+    for (int sp = 0; sp < 2; sp++) W.Nn[sp] = take(a->cap);
+    for (int sp = 0; sp < 2; sp++) W.Ll[sp] = take(a->cap);
+    W.vscale = take(a->cap);
+    W.id = reinterpret_cast<long long*>(take(a->cap));
+    return W;
 }
 
 // device arrays for a recorded run of nsteps with checkpoints every interval
@@ -493,6 +854,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
     const long long cap = ctx->cap;
     const int NS = ctx->NS;
     const int nck = (nsteps + interval - 1) / interval;
+    const long long nm = mesh_elems(ctx);
     emu_adjoint* a = ctx->adj;
     if (a && (a->cap != cap || a->NS != NS || a->ck_slots < nck || a->seg_slots < interval ||
               (int)a->dts.size() < nsteps)) {
@@ -507,24 +869,38 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         a->dts.resize(std::max(nsteps, 1));
         a->ck_slots = std::max(nck, 1);
         a->seg_slots = interval;
+        a->resorted.assign(a->ck_slots, 0);
         const size_t slot = (size_t)(NS + 3) * cap;
+        // stage states and meshes of every step of a segment when they take
+        // at most a quarter of the free memory (and 16 GiB); otherwise one
+        // step's worth, recomputed step by step
+        size_t fre = 0, tot = 0;
+        cudaMemGetInfo(&fre, &tot);
+        size_t budget = std::min(fre / 4, (size_t)16 << 30);
+        if (const char* env = std::getenv("EMU_ADJOINT_STORE_MAX_BYTES")) budget = (size_t)std::strtoull(env, nullptr, 10);
+        const size_t per_step = sizeof(double) * ((size_t)4 * NS * cap + (size_t)4 * nm);
+        a->store = (size_t)interval * per_step <= budget;
+        const size_t st_steps = a->store ? (size_t)interval : 1;
         CU(cudaMalloc(&a->dts_dev, sizeof(double) * a->dts.size()));
         CU(cudaMalloc(&a->ck, sizeof(double) * slot * a->ck_slots));
         CU(cudaMalloc(&a->seg, sizeof(double) * slot * a->seg_slots));
-        // Y2..Y4, Yn, acc, lamY0, lamn, lamYd, wf: 9 NS; lamN 2; wpos 3; wtime 1
-        CU(cudaMalloc(&a->work, sizeof(double) * (size_t)(9 * NS + 6) * cap));
-        for (int i = 0; i < 4; i++) CU(cudaMalloc(&a->lmesh[i], sizeof(double) * mesh_elems(ctx)));
+        CU(cudaMalloc(&a->perm, sizeof(unsigned) * cap * a->ck_slots));
+        CU(cudaMalloc(&a->stat, (size_t)2 * 13 * 8 * cap));
+        CU(cudaMalloc(&a->sst, sizeof(double) * st_steps * 4 * NS * cap));
+        CU(cudaMalloc(&a->mst, sizeof(double) * st_steps * 4 * nm));
+        // acc, lamY0, lamn, lamYd, wf, lamtmp: 6 NS; lamN 2, lamtmp 2; wpos 3; wtime 1
+        CU(cudaMalloc(&a->work, sizeof(double) * (size_t)(6 * NS + 8) * cap));
+        for (int i = 0; i < 4; i++) CU(cudaMalloc(&a->lmesh[i], sizeof(double) * nm));
         CU(cudaMalloc(&a->nex, sizeof(double) * 2 * ctx->P.ncells));
         CU(cudaMalloc(&a->rows, sizeof(double) * (size_t)NS * cap));
         double* w = a->work;
-        for (int s = 2; s <= 4; s++) { a->Y[s] = w; w += (size_t)NS * cap; }
-        a->Yn = w; w += (size_t)NS * cap;
         a->acc = w; w += (size_t)NS * cap;
         a->lamY0 = w; w += (size_t)NS * cap;
+        a->lamN = w; w += (size_t)2 * cap;        // lamN follows lamY0: one (NS+2) x cap block
         a->lamn = w; w += (size_t)NS * cap;
         a->lamYd = w; w += (size_t)NS * cap;
         a->wf = w; w += (size_t)NS * cap;
-        a->lamN = w; w += (size_t)2 * cap;
+        a->lamtmp = w; w += (size_t)(NS + 2) * cap;
         a->wpos = w; w += (size_t)3 * cap;
         a->wtime = w;
     }
@@ -540,22 +916,12 @@ double* slot_x(emu_adjoint* a, double* base, long long i, int d)
     return slot_f(a, base, i) + (size_t)(a->NS + d) * a->cap;
 }
 
-// copy (f, x) of a DevState-like view into a slot and back
 int save_slot(emu_context* ctx, emu_adjoint* a, double* base, long long i, const double* f, double* const pos[3])
 {
     const size_t fb = sizeof(double) * (size_t)a->NS * a->cap, xb = sizeof(double) * a->cap;
     CU(cudaMemcpyAsync(slot_f(a, base, i), f, fb, cudaMemcpyDeviceToDevice, ctx->stream));
     for (int d = 0; d < 3; d++)
         CU(cudaMemcpyAsync(slot_x(a, base, i, d), pos[d], xb, cudaMemcpyDeviceToDevice, ctx->stream));
-    return EMU_OK;
-}
-
-int load_slot(emu_context* ctx, emu_adjoint* a, double* base, long long i, double* f, double* const pos[3])
-{
-    const size_t fb = sizeof(double) * (size_t)a->NS * a->cap, xb = sizeof(double) * a->cap;
-    CU(cudaMemcpyAsync(f, slot_f(a, base, i), fb, cudaMemcpyDeviceToDevice, ctx->stream));
-    for (int d = 0; d < 3; d++)
-        CU(cudaMemcpyAsync(pos[d], slot_x(a, base, i, d), xb, cudaMemcpyDeviceToDevice, ctx->stream));
     return EMU_OK;
 }
 
@@ -574,6 +940,42 @@ int deposit_into(emu_context* ctx, const DevState& S, const double* f, double* m
     CU(cudaMemsetAsync(mesh, 0, sizeof(double) * mesh_elems(ctx), ctx->stream));
     emu::launch_deposit(ctx->nf, ctx->P, S, f, mesh, ctx->stream);
     return check_launch(ctx, "adjoint deposit");
+}
+
+// forward over steps [0, len) of G (step 0's Y_0, x in place, stored meshes
+// zeroed), storing stage states and meshes, then the backward sweep
+int segment_sweep(emu_context* ctx, const DevState& W, const emu::SegPtrs& G, bool coop)
+{
+    const int nf = ctx->nf;
+    const long long cap = ctx->cap;
+    cudaStream_t st = ctx->stream;
+    int r;
+    if ((r = deposit_into(ctx, emu::seg_state(W, G, 0), emu::seg_f(G, 0), emu::seg_m(G, 0, 0)))) return r;
+    if (coop) {
+        cudaError_t e = emu::launch_adj_seg_coop(nf, true, ctx->P, W, G, ctx->ctl, st);
+        if (e == cudaSuccess) e = emu::launch_adj_seg_coop(nf, false, ctx->P, W, G, ctx->ctl, st);
+        if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("adjoint segment: ") + cudaGetErrorString(e));
+        return check_launch(ctx, "adjoint segment");
+    }
+    for (int j = 0; j < G.len; j++) {
+        const DevState Q = emu::seg_state(W, G, j);
+        const double dt = ctx->adj->dts[G.k0 + j];
+        const double* Y0 = emu::seg_f(G, j);
+        for (int s = 1; s <= 3; s++)
+            emu::launch_adj_fwd_stage(nf, ctx->P, Q, s, dt, s == 1 ? Y0 : emu::seg_y(G, j, s, cap), Y0, G.acc,
+                                      emu::seg_y(G, j, s + 1, cap), emu::seg_m(G, j, s - 1), emu::seg_m(G, j, s), st);
+        const bool more = j + 1 < G.len;
+        emu::launch_adj_fwd_stage4_next(nf, ctx->P, Q, dt, emu::seg_y(G, j, 4, cap), G.acc, emu::seg_y(G, j, 5, cap),
+                                        more ? emu::seg_f(G, j + 1) : nullptr,
+                                        more ? emu::seg_f(G, j + 1) + (long long)G.NS * cap : nullptr,
+                                        emu::seg_m(G, j, 3), more ? emu::seg_m(G, j + 1, 0) : nullptr, st);
+    }
+    for (int j = G.len - 1; j >= 0; j--) {
+        const DevState Q = emu::seg_state(W, G, j);
+        const double dt = ctx->adj->dts[G.k0 + j];
+        for (int s = 4; s >= 0; s--) emu::launch_adj_stage(nf, ctx->P, Q, s, dt, emu::seg_stage_ptrs(G, j, s, cap), st);
+    }
+    return check_launch(ctx, "adjoint segment");
 }
 
 }  // namespace
@@ -600,15 +1002,25 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
     a->recorded = false;
     ctx->adj_valid = false;
     a->t0 = start_time;
+    std::fill(a->resorted.begin(), a->resorted.end(), 0);
     if ((r = emu_evolve_begin(ctx, start_time, INFINITY, nsteps))) return r;
-    const DevState& S = ctx->S[ctx->cur];
+    emu::launch_ctl_hist(ctx->ctl, a->dts_dev, ctx->stream);   // the step kernels record their dt
     for (int k = 0; k < nsteps; k++) {
-        if (k % checkpoint_interval == 0 &&
-            (r = save_slot(ctx, a, a->ck, k / checkpoint_interval, S.f0, S.pos)))
-            return r;
-        CU(cudaMemcpyAsync(a->dts_dev + k, &ctx->ctl->dt, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        if (k % checkpoint_interval == 0) {
+            const int c = k / checkpoint_interval;
+            // cell re-sort at segment starts only: the order is fixed inside a
+            // segment; the backward undoes the permutation at the boundary
+            if (c > 0 && ctx->prm.resort_interval > 0) {
+                if ((r = emu_ctx::resort_now(ctx, a->perm + (size_t)c * a->cap))) return r;
+                a->resorted[c] = 1;
+            }
+            const DevState& S = ctx->S[ctx->cur];
+            if ((r = save_slot(ctx, a, a->ck, c, S.f0, S.pos))) return r;
+        }
         if ((r = emu_ctx::step_device(ctx))) return r;
     }
+    emu::launch_ctl_hist(ctx->ctl, nullptr, ctx->stream);
+    ctx->steps_since_sort = 0;
     emu_run_info ri{};
     r = emu_evolve_end(ctx, &ri);
     if (info) *info = ri;
@@ -640,14 +1052,13 @@ int emu_adjoint_objective(emu_context* ctx, double* J, double* lam_f, double* la
     if ((r = deposit_into(ctx, S, S.f0, mesh))) return r;
     CU(cudaMemsetAsync(lm, 0, sizeof(double) * mesh_elems(ctx), ctx->stream));
     emu::launch_adj_nex(ctx->nf, ctx->P, mesh, lm, a->nex, ctx->stream);
-    double* lamf = a->Yn;         // scratch
-    double* lamN = a->lamN;
+    double* lamf = a->lamtmp;   // scratch
+    double* lamN = a->lamtmp + (size_t)ctx->NS * cap;
     emu::launch_adj_gather(ctx->nf, ctx->P, S, lm, lamf, lamN, ctx->stream);
     if ((r = check_launch(ctx, "adjoint objective"))) return r;
     std::vector<double> nex((size_t)2 * nc);
     CU(cudaMemcpyAsync(nex.data(), a->nex, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost, ctx->stream));
     const unsigned g = (unsigned)((n + emu::kBlock - 1) / emu::kBlock);
-    std::vector<double> tmpN;
     if (lam_f) {
         emu::k_soa_to_rows<<<g, emu::kBlock, 0, ctx->stream>>>(S.id, lamf, ctx->NS, cap, n, a->rows);
         CU(cudaMemcpyAsync(lam_f, a->rows, sizeof(double) * (size_t)n * ctx->NS, cudaMemcpyDeviceToHost,
@@ -684,7 +1095,7 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
     const unsigned g = (unsigned)((n + emu::kBlock - 1) / emu::kBlock);
     const long long nm = mesh_elems(ctx);
 
-    // adjoint state of the final (renormalised) state, in slot order
+    // adjoint state of the final (renormalised) state, in the final slot order
     CU(cudaMemcpyAsync(a->rows, lam_f_final, sizeof(double) * (size_t)n * NS, cudaMemcpyHostToDevice, st));
     emu::k_rows_to_soa<<<g, emu::kBlock, 0, st>>>(S.id, a->rows, NS, cap, n, a->lamY0);
     CU(cudaStreamSynchronize(st));
@@ -694,70 +1105,95 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
     } else {
         CU(cudaMemsetAsync(a->lamN, 0, sizeof(double) * 2 * cap, st));
     }
+    // working copy of the static fields, carried back through the re-sorts
+    int w = 0;
+    emu::k_static_scatter<<<g, emu::kBlock, 0, st>>>(S, stat_view(a, 0, S), nullptr, nullptr, nullptr, 0);
     CU(cudaMemsetAsync(a->lmesh[0], 0, sizeof(double) * nm, st));
+    emu::launch_ctl_set(ctx->ctl, 0.0, 0.0, INFINITY, INT_MAX, 0, st);
     if ((r = check_launch(ctx, "adjoint input"))) return r;
+    const bool coop = a->store && emu::adj_coop_fits(nf, ctx->P, n);
 
-    // recompute view: the run's static fields with private state arrays
-    DevState R = S;
-    R.f0 = a->wf;
-    for (int d = 0; d < 3; d++) R.pos[d] = a->wpos + (size_t)d * cap;
-    R.time = a->wtime;
-    double* const wpos[3] = {R.pos[0], R.pos[1], R.pos[2]};
-    double* const* M = ctx->mesh;   // M_1..M_4 live in mesh[0..3]
+    emu::SegPtrs G{};
+    G.seg_stride = (long long)(NS + 3) * cap;
+    G.sst = a->sst;
+    G.mst = a->mst;
+    G.sst_stride = a->store ? (long long)4 * NS * cap : 0;
+    G.mst_stride = a->store ? 4 * nm : 0;
+    G.dts = a->dts_dev;
+    G.NS = NS;
+    G.acc = a->acc;
+    for (int i = 0; i < 4; i++) G.lm[i] = a->lmesh[i];
+    G.nmesh = nm;
+    G.lamY0 = a->lamY0;
+    G.lamn = a->lamn;
+    G.lamYd = a->lamYd;
+    G.lamN = a->lamN;
 
     for (int seg = a->nck - 1; seg >= 0; seg--) {
-        const int k0 = seg * a->interval, k1 = std::min(k0 + a->interval, a->nsteps);
-        // forward over the segment from its checkpoint, saving (Y_0, x) per step
-        if ((r = load_slot(ctx, a, a->ck, seg, a->wf, wpos))) return r;
-        CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
-        if ((r = deposit_into(ctx, R, R.f0, M[0]))) return r;
-        for (int k = k0; k < k1; k++) {
-            if ((r = save_slot(ctx, a, a->seg, k - k0, a->wf, wpos))) return r;
-            if (k + 1 < k1) {
-                emu::launch_ctl_set(ctx->ctl, a->dts[k], 0.0, INFINITY, INT_MAX, 0, st);
+        const int k0 = seg * a->interval, k1 = std::min(k0 + a->interval, a->nsteps), len = k1 - k0;
+        DevState W = stat_view(a, w, S);   // static fields in this segment's slot order
+        W.fs = S.fs;
+        W.acc = S.acc;
+        if (a->store) {
+            G.seg = a->seg;
+            G.k0 = k0;
+            G.len = len;
+            CU(cudaMemcpyAsync(a->seg, slot_f(a, a->ck, seg), sizeof(double) * G.seg_stride, cudaMemcpyDeviceToDevice,
+                               st));
+            CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * (size_t)len * 4 * nm, st));
+            if ((r = segment_sweep(ctx, W, G, coop))) return r;
+        } else {
+            // (Y_0, x) of every step of the segment, then each step as a
+            // one-step segment (its stage states recomputed)
+            DevState R = W;
+            R.f0 = a->wf;
+            for (int d = 0; d < 3; d++) R.pos[d] = a->wpos + (size_t)d * cap;
+            R.time = a->wtime;
+            double* const* M = ctx->mesh;
+            CU(cudaMemcpyAsync(a->wf, slot_f(a, a->ck, seg), sizeof(double) * NS * cap, cudaMemcpyDeviceToDevice, st));
+            CU(cudaMemcpyAsync(a->wpos, slot_x(a, a->ck, seg, 0), sizeof(double) * 3 * cap, cudaMemcpyDeviceToDevice,
+                               st));
+            CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
+            if ((r = deposit_into(ctx, R, R.f0, M[0]))) return r;
+            for (int k = k0; k < k1; k++) {
+                emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(R, slot_f(a, a->seg, k - k0), NS, a->dts_dev, k, ctx->ctl);
+                if (k + 1 == k1) break;
                 for (int s = 1; s <= 4; s++)
                     emu::launch_rk4_stage(nf, ctx->P, R, s, M[s - 1], M[s % 4], M[(s + 1) % 4], nm, ctx->ctl, -1, st);
             }
-        }
-        if ((r = check_launch(ctx, "adjoint segment recompute"))) return r;
-        // backward through the segment's steps
-        for (int k = k1 - 1; k >= k0; k--) {
-            const double dt = a->dts[k];
-            DevState Q = S;   // weights from the step's start positions
-            for (int d = 0; d < 3; d++) Q.pos[d] = slot_x(a, a->seg, k - k0, d);
-            const double* Y0 = slot_f(a, a->seg, k - k0);
-            const double* Ys[5] = {Y0, Y0, a->Y[2], a->Y[3], a->Y[4]};
-            for (int i = 1; i < 4; i++) CU(cudaMemsetAsync(M[i], 0, sizeof(double) * nm, st));
-            if ((r = deposit_into(ctx, Q, Y0, M[0]))) return r;
-            for (int s = 1; s <= 4; s++)
-                emu::launch_adj_fwd_stage(nf, ctx->P, Q, s, dt, Ys[s], Y0, a->acc, s < 4 ? a->Y[s + 1] : a->Yn,
-                                          M[s - 1], s < 4 ? M[s] : nullptr, st);
-            for (int s = 4; s >= 0; s--) {
-                emu::AdjStagePtrs A{};
-                A.Ys = s >= 1 ? Ys[s] : nullptr;
-                A.Ynext = s < 4 ? Ys[s + 1] : nullptr;
-                A.Yn = a->Yn;
-                A.mesh_s = s >= 1 ? M[s - 1] : nullptr;
-                A.lm_in = s < 4 ? a->lmesh[(s + 1) % 4] : nullptr;
-                A.lm_out = s >= 1 ? a->lmesh[s % 4] : nullptr;
-                A.lm_zero = s >= 1 ? a->lmesh[(s + 3) % 4] : nullptr;
-                A.nmesh = nm;
-                A.lamY0 = a->lamY0;
-                A.lamn = a->lamn;
-                A.lamYd = a->lamYd;
-                A.lamN = a->lamN;
-                emu::launch_adj_stage(nf, ctx->P, Q, s, dt, A, st);
+            if ((r = check_launch(ctx, "adjoint segment recompute"))) return r;
+            for (int k = k1 - 1; k >= k0; k--) {
+                G.seg = slot_f(a, a->seg, k - k0);
+                G.k0 = k;
+                G.len = 1;
+                CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * 4 * nm, st));
+                if ((r = segment_sweep(ctx, W, G, false))) return r;
             }
-            if ((r = check_launch(ctx, "adjoint step"))) return r;
+        }
+        if (seg > 0 && a->resorted[seg]) {
+            // undo the re-sort made at the start of this segment
+            const unsigned* perm = a->perm + (size_t)seg * cap;
+            emu::k_static_scatter<<<g, emu::kBlock, 0, st>>>(W, stat_view(a, 1 - w, S), perm, a->lamY0, a->lamtmp,
+                                                             NS + 2);
+            CU(cudaMemcpyAsync(a->lamY0, a->lamtmp, sizeof(double) * (size_t)(NS + 2) * cap, cudaMemcpyDeviceToDevice,
+                               st));
+            w = 1 - w;
         }
     }
-    // outputs in load order
-    emu::k_soa_to_rows<<<g, emu::kBlock, 0, st>>>(S.id, a->lamY0, NS, cap, n, a->rows);
+    CU(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if ((r = check_launch(ctx, "adjoint sweep"))) return r;
+    if (ctx->ctl_host->status & EMU_ERR_TIMEOUT)
+        return fail(ctx, EMU_ERR_TIMEOUT, "emu_adjoint_backward: a grid barrier timed out");
+    // outputs in load order (the order of the run's first segment)
+    const DevState W0 = stat_view(a, w, S);
+    emu::k_soa_to_rows<<<g, emu::kBlock, 0, st>>>(W0.id, a->lamY0, NS, cap, n, a->rows);
     CU(cudaMemcpyAsync(lam_f0, a->rows, sizeof(double) * (size_t)n * NS, cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
-    emu::k_soa_to_rows<<<g, emu::kBlock, 0, st>>>(S.id, a->lamN, 2, cap, n, a->rows);
+    emu::k_soa_to_rows<<<g, emu::kBlock, 0, st>>>(W0.id, a->lamN, 2, cap, n, a->rows);
     CU(cudaMemcpyAsync(lam_N0, a->rows, sizeof(double) * (size_t)n * 2, cudaMemcpyDeviceToHost, st));
     // the forward meshes were reused: restore the current state's deposit
+    double* const* M = ctx->mesh;
     CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
     if ((r = deposit_into(ctx, S, S.f0, M[0]))) return r;
     ctx->cur_mesh = 0;

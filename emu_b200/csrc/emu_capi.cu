@@ -405,6 +405,16 @@ int emu_ctx::step_device(emu_context* ctx)
     return EMU_OK;
 }
 
+int emu_ctx::resort_now(emu_context* ctx, unsigned* perm)
+{
+    int r;
+    if ((r = resort(ctx))) return r;
+    if (perm)
+        CU(cudaMemcpyAsync(perm, ctx->idx2, sizeof(unsigned) * ctx->S[ctx->cur].n, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    return EMU_OK;
+}
+
 extern "C" {
 
 int emu_abi_version(void) { return EMU_B200_ABI_VERSION; }

@@ -59,6 +59,9 @@ int check_launch(emu_context* ctx, const char* what);
 // one device-resident step of the fused RK4 loop (cooperative kernel or
 // graph), without the periodic re-sort; dt comes from the device control
 int step_device(emu_context* ctx);
+// re-sort the particles by cell now; when perm is not null it receives the
+// gather permutation (new slot i holds old slot perm[i])
+int resort_now(emu_context* ctx, unsigned* perm);
 // frees the adjoint arrays (emu_destroy)
 void adjoint_free(emu_context* ctx);
 

@@ -172,6 +172,8 @@ void launch_q_to_f64(int nf, const DevParams& P, const long long* mesh, double* 
     EMU_NF_DISPATCH(nf, (k_q_to_f64<NFv><<<grid_for(P.ncells * 8 * NFv * NFv), kBlock, 0, st>>>(P, mesh, out)));
 }
 
+void launch_ctl_hist(StepCtl* ctl, double* hist, cudaStream_t st) { k_ctl_hist<<<1, 1, 0, st>>>(ctl, hist); }
+
 void launch_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status,
                     cudaStream_t st)
 {

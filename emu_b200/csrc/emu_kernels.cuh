@@ -58,6 +58,7 @@ struct StepCtl {
     unsigned int blocks_done;
     unsigned long long vmax_bits[2];   // max V_adaptive, V_stupid (non-negative doubles as bits)
     unsigned int bar_count, bar_gen;   // grid barrier of the cooperative step kernel
+    double* dt_hist;     // when set: dt of step k is written to dt_hist[k] (recorded runs)
 };
 
 enum DtMode : int { DT_QUERY = 0, DT_INIT = 1, DT_ADVANCE = 2 };
@@ -101,6 +102,7 @@ void launch_renorm(int nf, const DevParams& P, const DevState& S, StepCtl* ctl, 
 void launch_mesh_out(int nf, const DevParams& P, const double* mesh, double* out, cudaStream_t st);
 void launch_mesh_out_q(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st);
 void launch_q_to_f64(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st);
+void launch_ctl_hist(StepCtl* ctl, double* hist, cudaStream_t st);
 void launch_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status,
                     cudaStream_t st);
 void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st);

@@ -116,6 +116,12 @@ __device__ __forceinline__ void report_bad(StepCtl* ctl, int st, long long id)
     }
 }
 
+// recorded runs: the dt of the step in progress goes to dt_hist[step]
+__device__ __forceinline__ void record_dt(StepCtl* ctl, double dt)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ctl->dt_hist) ctl->dt_hist[ctl->step] = dt;
+}
+
 // grid-stride zeroing fused into a kernel
 template <class T>
 __device__ __forceinline__ void zero_slice(T* buf, long long n)
@@ -457,6 +463,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S
     const int done = ctl->done;
     const double dt = ctl->dt;   // both control loads in one round trip
     if (done) return;
+    if (s == 1) record_dt(ctl, dt);
     rk4_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt);
     // stage 4 of the device-resident loop: compute_dt on the stage-4 mesh
     // (main.cpp:193-198), which this kernel only reads
@@ -507,6 +514,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_step_coop(DevParams P, DevSta
     const int done = ctl->done;
     const double dt = ctl->dt;
     if (done) return;
+    record_dt(ctl, dt);
     rk4_stage_body<NF, SWt>(P, S, 1, m0, m1, m2, nmesh, ctl, dt);
     grid_barrier(ctl);
     rk4_stage_body<NF, SWt>(P, S, 2, m1, m2, m3, nmesh, ctl, dt);
@@ -1024,6 +1032,8 @@ __global__ void k_q_to_f64(DevParams P, const long long* __restrict__ mesh, doub
     out[i] = (double)mesh[i] * P.q_unscale[((int)(i % ND) / NH) & 1];
 }
 
+__global__ void k_ctl_hist(StepCtl* ctl, double* hist) { ctl->dt_hist = hist; }
+
 __global__ void k_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status)
 {
     ctl->dt = dt;
@@ -1037,6 +1047,7 @@ __global__ void k_ctl_set(StepCtl* ctl, double dt, double t, double end_time, in
     ctl->vmax_bits[0] = ctl->vmax_bits[1] = 0ull;
     ctl->bar_count = 0u;
     ctl->bar_gen = 0u;
+    ctl->dt_hist = nullptr;
     if (reset_status) {
         ctl->status = 0;
         ctl->bad = LLONG_MAX;

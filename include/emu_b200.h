@@ -259,8 +259,12 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * (lam_f_final, n x 2nf^2) and optionally dJ/d(N, Nbar) taken at the final
  * state (lam_N_final, n x 2, NULL = 0), the gradient with respect to the
  * run's initial f (lam_f0) and N, Nbar (lam_N0), with the recorded dt held
- * fixed.  Recomputes each checkpoint segment and each step's stages.  The
- * context's particle state is unchanged.
+ * fixed.  Recomputes each checkpoint segment from its checkpoint; the stage
+ * states and meshes of a whole segment are kept when they fit a budget
+ * (a quarter of the free device memory, at most 16 GiB; environment variable
+ * EMU_ADJOINT_STORE_MAX_BYTES overrides it), else each step's stages are
+ * recomputed before its backward step.  The context's particle state is
+ * unchanged.
  */
 int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, double start_time, double* dts,
                         emu_run_info* info);

@@ -149,3 +149,25 @@ def test_adjoint_errors():
         c.load_particles(parts)
         with pytest.raises(api.EmuError):
             c.adjoint_forward(3, 2)
+
+
+@pytest.mark.parametrize("store", ["segment", "per_step"])
+def test_adjoint_memory_modes_agree(monkeypatch, store):
+    """stage states kept for a whole segment, or recomputed step by step
+    (budget 0): same gradient to rounding"""
+    if store == "per_step":
+        monkeypatch.setenv("EMU_ADJOINT_STORE_MAX_BYTES", "0")
+    p = W.c2_fast_flavor_1d(ncell_z=8, ndirs=6)
+    parts = api.init_particles(p)
+    fc, nc = flavor_columns(2), number_columns(2)
+    with AdjointRun(p, parts, 7, 3) as run:
+        run.forward(parts[:, fc], parts[:, nc])
+        J, lf, lN = run.ctx.adjoint_objective()
+        g, gN = run.ctx.adjoint_backward(lf, lN)
+        dts = run.dts
+    te = TorchEmu(p, parts)
+    f0r = torch.tensor(parts[:, fc], requires_grad=True)
+    Nr = torch.tensor(parts[:, nc], requires_grad=True)
+    te.loss(f0r, Nr, dts).backward()
+    assert _rel(g, f0r.grad.numpy()) < 1e-9
+    assert _rel(gN, Nr.grad.numpy()) < 1e-9
