@@ -1,10 +1,11 @@
-"""Build the CUDA library libemu_b200.so in-tree (sm_100a).
+"""Build the CUDA library libemu_b200.so in-tree (sm_100a) and the host
+driver emu_main that runs the reference's inputs files through it.
 
     python -m emu_b200.build [--force] [--verbose-ptxas]
 
 Objects go to emu_b200/_build/, the shared library to emu_b200/libemu_b200.so
-(next to this file, so it travels with the source tree).  nvcc cross-compiles
-without a GPU.
+and the driver to emu_b200/emu_main (next to this file, so both travel with
+the source tree).  nvcc cross-compiles without a GPU.
 """
 import concurrent.futures as cf
 import os
@@ -16,6 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libemu_b200.so")
+MAIN = os.path.join(HERE, "emu_main")
 INCLUDE = os.path.join(ROOT, "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -71,6 +73,13 @@ def build(force=False, verbose_ptxas=False, quiet=True):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    main_src = os.path.join(CSRC, "emu_main.cpp")
+    if force or _stale(MAIN, [main_src, LIB, os.path.join(INCLUDE, "emu_b200.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, main_src, "-o", MAIN, "-L", HERE, "-lemu_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("emu_main build failed:\n%s\n%s" % (r.stdout, r.stderr))
     return LIB, logs
 
 
