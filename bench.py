@@ -39,13 +39,15 @@ from emu_b200 import workloads as W  # noqa: E402
 METRIC = "particle RK4 steps/s on 1 B200: mixed vs FP64 at stated err; % of HBM peak"
 
 
-def workload(name, precision, cells=None, fused=None, resort=None):
+def workload(name, precision, cells=None, fused=None, resort=None, ranks=1):
     """cells overrides the cell count (z cells for c2/c3, cells per side for
-    c5) to run a smaller case of the same workload (profiling)."""
+    c5) to run a smaller case of the same workload (profiling).  With ranks
+    > 1 every cell gets ranks times the directions, so that each rank's
+    shard (every ranks-th particle) has the single-GPU particle count."""
     if name == "c2":
-        p = W.c2_fast_flavor_1d(ncell_z=cells or 128)
-        desc = "C2 fast-flavor 1D: 2 flavors, 1x1x%d cells over %g cm, 80 Fibonacci directions/cell" % (
-            p.ncell[2], p.Lz)
+        p = W.c2_fast_flavor_1d(ncell_z=cells or 128, ndirs=80 * ranks)
+        desc = "C2 fast-flavor 1D: 2 flavors, 1x1x%d cells over %g cm, %d Fibonacci directions/cell" % (
+            p.ncell[2], p.Lz, 80 * ranks)
     elif name == "c4":
         p = W.c4_adjoint()
         desc = ("C4 adjoint: C2 sizes (2 flavors, 1x1x%d cells, 80 directions/cell), %d RK4 steps, "
@@ -53,9 +55,12 @@ def workload(name, precision, cells=None, fused=None, resort=None):
     elif name == "c3":
         p = W.c3_three_flavor_1d(ncell_z=cells or 1024)
         desc = "C3 3-flavor 1D: 1x1x%d cells, 378 ring directions/cell" % p.ncell[2]
+        if ranks > 1:
+            p.direction_generator, p.ndirections = 1, 378 * ranks
+            desc = "C3 3-flavor 1D: 1x1x%d cells, %d Fibonacci directions/cell" % (p.ncell[2], 378 * ranks)
     elif name == "c5":
-        p = W.c5_3d(n=cells or 64)
-        desc = "C5 3-flavor 3D: %d^3 cells x 96 Fibonacci directions" % p.ncell[0]
+        p = W.c5_3d(n=cells or 64, ndirs=96 * ranks)
+        desc = "C5 3-flavor 3D: %d^3 cells x %d Fibonacci directions" % (p.ncell[0], 96 * ranks)
     else:
         raise SystemExit("unknown workload " + name)
     if precision:
@@ -213,18 +218,30 @@ def run_emu(args):
     import torch
     ws, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
-    if ws > 1:
+    if ws > 1 or args.sharded:
         import datetime
         import torch.distributed as dist
+        if ws == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29533")
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    p, desc = workload(args.workload, args.precision, args.cells, args.fused, args.resort)
+    multi = (ws > 1 or args.sharded) and args.workload != "c4"
+    p, desc = workload(args.workload, args.precision, args.cells, args.fused, args.resort, ws if multi else 1)
     mixed = p.precision == api.PREC_MIXED
     nf = p.nflavors
     recs = api.init_particles(p)
-    n = recs.shape[0]
     stream = torch.cuda.Stream()
     ctx = api.Context(p)
     ctx.set_stream(stream.cuda_stream)
+    if multi:
+        # particle sharding: this rank's particles, replicated mesh summed
+        # over the ranks by an NCCL all-reduce after every deposit
+        from emu_b200 import sharding
+        sharding.attach(ctx, rank, ws)
+        recs = sharding.shard(recs, rank, ws)
+    n = recs.shape[0]
     ctx.load_particles(recs)
     total_steps = args.warmup + args.steps + args.profile_steps + 8
     ctx.evolve_begin(0.0, float("inf"), total_steps)
@@ -334,7 +351,8 @@ def run_emu(args):
         "config": {"workload": desc, "particles": n, "nflavors": nf, "cells": list(p.ncell),
                    "precision": "mixed" if mixed else "fp64", "integrator": "RK4",
                    "l2": "flushed (512 MB write) before every timed step",
-                   "parallelism": "replica per GPU" if ws > 1 else "1 GPU",
+                   "parallelism": ("particles sharded over %d GPUs, replicated mesh, NCCL all-reduce of "
+                                   "every deposit" % ws) if multi else ("replica per GPU" if ws > 1 else "1 GPU"),
                    "resort_interval": p.resort_interval},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -348,12 +366,12 @@ def run_emu(args):
         "wall_s": wall,
         "kernel_ms_per_step": [float(x) for x in kms.mean(axis=0)],
     }
-    if args.workload == "c4":
+    if args.workload == "c4" and ws == 1:
         out["adjoint"] = run_adjoint(ctx, recs, p, stream, total_ms / args.steps)
     ctx.close()
     if rank == 0:
         print(json.dumps(out))
-    if ws > 1:
+    if torch.distributed.is_initialized():
         torch.distributed.destroy_process_group()
 
 
@@ -411,6 +429,8 @@ def main():
                     help="RK4 kernels: 2 one cooperative launch per step when it fits (default), 1 per stage")
     ap.add_argument("--resort", type=int, default=None,
                     help="steps between on-device cell re-sorts (0 never; default the workload's)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="particle-sharded path even on one GPU (a one-rank communicator)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=15.0)

@@ -130,11 +130,24 @@ SIGNATURES = {
     "emu_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "emu_deposit_noalloc": (ctypes.c_int, [_P(EmuParams), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "emu_comm_id": (ctypes.c_int, [ctypes.c_char_p]),
+    "emu_attach_comm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
     "emu_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D,
                                            _P(EmuRunInfo)]),
     "emu_adjoint_objective": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
     "emu_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D]),
 }
+
+
+COMM_ID_BYTES = 128
+
+
+def comm_id():
+    """a new communicator id (bytes) for Context.attach_comm"""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(COMM_ID_BYTES)
+    _check(lib.emu_comm_id(buf), None, "emu_comm_id")
+    return buf.raw
 
 
 def load_library(path=None):
@@ -344,6 +357,11 @@ class Context:
         if code & ~(EMU_ERR_TRACE | EMU_ERR_NEGDIAG | EMU_ERR_LENGTH | EMU_ERR_DT):
             self._ck(code, "emu_evolve")
         return info
+
+    def attach_comm(self, comm_id, rank, nranks):
+        """join a particle-sharding communicator (before load_particles)"""
+        assert len(comm_id) == COMM_ID_BYTES
+        self._ck(self.lib.emu_attach_comm(self.h, comm_id, int(rank), int(nranks)), "emu_attach_comm")
 
     # ---- discrete adjoint (FP64 RK4) ----
     def adjoint_forward(self, nsteps, checkpoint_interval, start_time=0.0):

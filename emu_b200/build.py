@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
 
 SOURCES = ["emu_k_fp64_3.cu", "emu_k_mixed_3.cu", "emu_adjoint.cu", "emu_k_fp64_2.cu", "emu_k_mixed_2.cu",
-           "emu_k_misc.cu", "emu_capi.cu", "emu_noalloc.cu", "emu_host.cpp", "emu_init.cpp"]
+           "emu_k_misc.cu", "emu_capi.cu", "emu_comm.cu", "emu_noalloc.cu", "emu_host.cpp", "emu_init.cpp"]
 HEADERS = ["emu_device.cuh", "emu_kernels.cuh", "emu_kernels_impl.cuh", "emu_context.cuh", "emu_host.h"]
 
 
@@ -69,7 +69,7 @@ def build(force=False, verbose_ptxas=False, quiet=True):
     if logs and not quiet:
         sys.stderr.write(logs)
     if force or _stale(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))

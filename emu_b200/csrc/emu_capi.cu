@@ -251,6 +251,9 @@ int deposit_current(emu_context* ctx)
     if (ctx->mixed) emu::launch_deposit_q(ctx->nf, ctx->P, S, S.f0, ctx->qmesh[0], ctx->stream);
     else emu::launch_deposit(ctx->nf, ctx->P, S, S.f0, ctx->mesh[0], ctx->stream);
     if ((r = check_launch(ctx, "deposit"))) return r;
+    if (ctx->mixed) r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[0], true, ctx->stream);
+    else r = emu_ctx::reduce_mesh(ctx, ctx->mesh[0], false, ctx->stream);
+    if (r) return r;
     ctx->cur_mesh = 0;
     ctx->fused_ready = true;
     return EMU_OK;
@@ -261,9 +264,12 @@ int deposit_current(emu_context* ctx)
 int enqueue_rk4_fp64(emu_context* ctx, cudaStream_t st, bool with_dt)
 {
     const DevState& S = ctx->S[ctx->cur];
-    for (int s = 1; s <= 4; s++)
+    int r;
+    for (int s = 1; s <= 4; s++) {
         emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4], ctx->mesh[(s + 1) % 4],
                               mesh_elems(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
+        if ((r = emu_ctx::reduce_mesh(ctx, ctx->mesh[s % 4], false, st))) return r;
+    }
     return check_launch(ctx, "rk4 stage");
 }
 
@@ -279,6 +285,8 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt)
         // step's first finalize zeroes it
         emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->qmesh[1], ctx->ctl,
                                     (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
+        int r;
+        if ((r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return r;
         a = b;
     }
     return check_launch(ctx, "rk4 mixed stage");
@@ -328,6 +336,7 @@ int step_generic(emu_context* ctx, double dt)
         }
         if ((r = zero_mesh(ctx, 0))) return r;
         emu::launch_deposit(ctx->nf, ctx->P, S, Y, ctx->mesh[0], ctx->stream);
+        if ((r = emu_ctx::reduce_mesh(ctx, ctx->mesh[0], false, ctx->stream))) return r;
         emu::launch_rhs(ctx->nf, ctx->P, S, Y, ctx->mesh[0], S.kgen + i * kstride, ctx->stream);
     }
     double w[4];
@@ -521,6 +530,7 @@ void emu_destroy(emu_context* ctx)
     if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
     if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
     emu_ctx::adjoint_free(ctx);
+    emu_ctx_comm_free(ctx);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     delete ctx;
@@ -553,12 +563,18 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
                        ctx->stream));
     // host-side scalars derived from the particles: Vvac_max (Init.cpp:657-660)
     // and, for the mixed path, the fixed-point scales
+    // (over all ranks of a sharded run)
     double vvac = 0.0;
     emu_vvac_max(&ctx->prm, records, n, &vvac);
+    if ((r = emu_ctx_reduce_scalars(ctx, &vvac, 1, 1))) return r;
     ctx->P.vvac_max = vvac;
     if (ctx->mixed) {
         std::string why;
-        if (!emu_host::fixed_point_scales(ctx->prm, records, n, ctx->P.q_scale, ctx->P.q_unscale, why))
+        double tot[2], mx[2];
+        emu_host::weight_totals(ctx->prm, records, n, tot, mx);
+        if ((r = emu_ctx_reduce_scalars(ctx, tot, 2, 0))) return r;
+        if ((r = emu_ctx_reduce_scalars(ctx, mx, 2, 1))) return r;
+        if (!emu_host::fixed_point_scales_from(tot, mx, ctx->P.q_scale, ctx->P.q_unscale, why))
             return fail(ctx, EMU_ERR_LIMIT, "emu_load_particles: " + why);
     }
     emu::launch_cell_keys(ctx->P, ctx->aos, ctx->nreal, n, ctx->keys, ctx->idx, ctx->stream);
@@ -572,7 +588,9 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     if ((r = check_launch(ctx, "pack"))) return r;
     free_graphs(ctx);   // kernel arguments (P, S) changed
     // fused == 2 (default): one cooperative launch per step when the grid fits
-    ctx->coop = !ctx->mixed && ctx->prm.fused == 2 && rk4_fused(ctx) && emu::coop_step_fits(ctx->nf, ctx->P, n);
+    // (a sharded run reduces every deposit between stages: per-stage kernels)
+    ctx->coop = !ctx->mixed && !ctx->comm && ctx->prm.fused == 2 && rk4_fused(ctx) &&
+                emu::coop_step_fits(ctx->nf, ctx->P, n);
     ctx->loaded = true;
     ctx->adj_valid = false;
     ctx->steps_since_sort = 0;
@@ -824,6 +842,8 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
                                         s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
+            int rr;
+            if ((rr = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return rr;
             a = b;
         }
     } else {
@@ -834,6 +854,8 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
                                   s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
+            int rr;
+            if ((rr = emu_ctx::reduce_mesh(ctx, ctx->mesh[s % 4], false, st))) return rr;
         }
     }
     int r = check_launch(ctx, "profile step");

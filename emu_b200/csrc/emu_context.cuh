@@ -46,6 +46,11 @@ struct emu_context {
     int steps_since_sort = 0;
     bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
     emu_adjoint* adj = nullptr;         // allocated by the first adjoint call
+    // particle sharding over ranks (emu_attach_comm): every deposit is summed
+    // over the ranks before a stage reads it
+    void* comm = nullptr;               // ncclComm_t
+    int rank = 0, nranks = 1;
+    double* red_scratch = nullptr;      // device scalars for load-time reductions
     bool adj_valid = false;             // a recorded run matches the slot order
     std::string err;
 };
@@ -59,6 +64,15 @@ int check_launch(emu_context* ctx, const char* what);
 // one device-resident step of the fused RK4 loop (cooperative kernel or
 // graph), without the periodic re-sort; dt comes from the device control
 int step_device(emu_context* ctx);
+// sum a deposited mesh (FP64, or int64 for the mixed path) over the ranks of
+// the attached communicator, enqueued on st; no-op without one
+int reduce_mesh(emu_context* ctx, void* mesh, bool int64, cudaStream_t st);
+}  // namespace emu_ctx
+// sum (op 0) or max (op 1) of n <= 8 host scalars over the ranks (synchronous)
+int emu_ctx_reduce_scalars(emu_context* ctx, double* v, int n, int op);
+// destroys the attached communicator (emu_destroy, after the graphs)
+void emu_ctx_comm_free(emu_context* ctx);
+namespace emu_ctx {
 // re-sort the particles by cell now; when perm is not null it receives the
 // gather permutation (new slot i holds old slot perm[i])
 int resort_now(emu_context* ctx, unsigned* perm);

@@ -150,18 +150,33 @@ void vacuum_m2(const emu_params& p, double m2[2][9])
         }
 }
 
-bool fixed_point_scales(const emu_params& p, const double* records, long long n, double scale[2], double unscale[2],
-                        std::string& why)
+void weight_totals(const emu_params& p, const double* records, long long n, double total[2], double mx[2])
 {
     const int nf = p.nflavors, nh = nf * nf, nr = 3 + 8 + 2 * (2 + nh);
     for (int s = 0; s < 2; s++) {
-        double total = 0.0, mx = 0.0;
+        total[s] = mx[s] = 0.0;
         const int off = 3 + 8 + s * (2 + nh);
         for (long long i = 0; i < n; i++) {
             const double v = std::fabs(records[i * nr + off]);
-            total += v;
-            if (v > mx) mx = v;
+            total[s] += v;
+            if (v > mx[s]) mx[s] = v;
         }
+    }
+}
+
+bool fixed_point_scales(const emu_params& p, const double* records, long long n, double scale[2], double unscale[2],
+                        std::string& why)
+{
+    double total[2], mx[2];
+    weight_totals(p, records, n, total, mx);
+    return fixed_point_scales_from(total, mx, scale, unscale, why);
+}
+
+bool fixed_point_scales_from(const double totals[2], const double maxima[2], double scale[2], double unscale[2],
+                             std::string& why)
+{
+    for (int s = 0; s < 2; s++) {
+        const double total = totals[s], mx = maxima[s];
         if (mx > 1e37) {
             why = "particle weight N above 1e37 does not fit the FP32 arithmetic of the mixed path";
             return false;

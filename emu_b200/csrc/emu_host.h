@@ -28,6 +28,11 @@ void vacuum_m2(const emu_params& p, double m2[2][9]);
 // integer with |sum over any cell| < 2^62 (bound: total N per species)
 bool fixed_point_scales(const emu_params& p, const double* records, long long n, double scale[2],
                         double unscale[2], std::string& why);
+// the same from per-species sums and maxima of |N| (summed / maxed over the
+// ranks of a sharded run first)
+void weight_totals(const emu_params& p, const double* records, long long n, double total[2], double mx[2]);
+bool fixed_point_scales_from(const double totals[2], const double maxima[2], double scale[2], double unscale[2],
+                             std::string& why);
 
 bool write_plotfile(const emu_params& p, const char* dir, double time, int step, const double* mesh,
                     const double* records, long long n, std::string& why);

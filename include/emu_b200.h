@@ -266,6 +266,27 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * recomputed before its backward step.  The context's particle state is
  * unchanged.
  */
+/*
+ * Particle sharding over GPUs (one process per GPU).  No counterpart in the
+ * reference, which distributes boxes of cells over MPI ranks.  Each rank
+ * creates its context, attaches it to a communicator, then loads its own
+ * disjoint subset of the particles; the mesh is replicated and every deposit
+ * is summed over the ranks (NCCL all-reduce on the context's stream) before
+ * any stage reads it, so every rank computes the same compute_dt and takes
+ * the same steps.  Vvac_max and the mixed path's fixed-point scales are
+ * reduced over the ranks at load.  The int64 mesh of the mixed path sums
+ * exactly (results independent of the rank count).  NCCL (libnccl.so.2) is
+ * loaded when first needed.
+ *   emu_comm_id: a new communicator id (EMU_COMM_ID_BYTES bytes), made on
+ *     one rank and handed to the others by the caller.
+ *   emu_attach_comm: joins it (collective over the nranks ranks); must
+ *     precede emu_load_particles.  nranks = 1 is allowed.
+ * Not available with the adjoint entry points.
+ */
+#define EMU_COMM_ID_BYTES 128
+int emu_comm_id(char* id);
+int emu_attach_comm(emu_context* ctx, const char* id, int rank, int nranks);
+
 int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, double start_time, double* dts,
                         emu_run_info* info);
 int emu_adjoint_objective(emu_context* ctx, double* J, double* lam_f, double* lam_N);

@@ -172,6 +172,18 @@ class Oracle(_Base):
         self.lib.oracle_shape(delta, order, ctypes.byref(first), w)
         return first.value, np.array(list(w))
 
+    def finish_step(self, parts):
+        """end of step in place: periodic wrap + position sync, then
+        Renormalize (main.cpp:163-170); returns the Renormalize status"""
+        assert parts.flags.c_contiguous and parts.dtype == np.float64
+        self.lib.oracle_wrap.argtypes = [ctypes.POINTER(OracleParams), _D, ctypes.c_int64]
+        self.lib.oracle_wrap(ctypes.byref(self.P), _ptr(parts), parts.shape[0])
+        bad = ctypes.c_int64(-1)
+        f = self._f("renormalize")
+        f.argtypes = [ctypes.POINTER(OracleParams), _D, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        f.restype = ctypes.c_int
+        return f(ctypes.byref(self.P), _ptr(parts), parts.shape[0], ctypes.byref(bad))
+
     def vvac(self, pupt):
         V = np.zeros(2 * self.nf * self.nf)
         self.lib.oracle_vvac.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_double, _D]
