@@ -243,6 +243,10 @@ def run_emu(args):
         recs = sharding.shard(recs, rank, ws)
     n = recs.shape[0]
     ctx.load_particles(recs)
+    # the library's automatic re-sort interval (resort_interval < 0)
+    eff_resort = p.resort_interval
+    if eff_resort < 0:
+        eff_resort = 1 if sum(1 for c in p.ncell if c > 1) == 3 and p.shape_order >= 2 else 4
     total_steps = args.warmup + args.steps + args.profile_steps + 8
     ctx.evolve_begin(0.0, float("inf"), total_steps)
     flush_bytes = 512 << 20
@@ -334,7 +338,7 @@ def run_emu(args):
         cpu = cpu_baseline(p, recs, args.cpu_budget, os.cpu_count() or 1)
 
     kernels_per_step = 1 if coop else (8 if mixed else 4)
-    resorts = (args.steps // p.resort_interval) if p.resort_interval > 0 else 0
+    resorts = (args.steps // eff_resort) if eff_resort > 0 else 0
     out = {
         "metric": METRIC,
         "value": value,
@@ -353,7 +357,7 @@ def run_emu(args):
                    "l2": "flushed (512 MB write) before every timed step",
                    "parallelism": ("particles sharded over %d GPUs, replicated mesh, NCCL all-reduce of "
                                    "every deposit" % ws) if multi else ("replica per GPU" if ws > 1 else "1 GPU"),
-                   "resort_interval": p.resort_interval},
+                   "resort_interval": eff_resort},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": kernel,
@@ -361,7 +365,10 @@ def run_emu(args):
                      "peak_source": peak_kind},
         "e2e": e2e,
         "cpu_baseline": cpu,
-        "gpu_launches": args.steps * kernels_per_step + 2 * resorts + args.steps,
+        # per step: the step kernels + the L2 flush; per re-sort: keys,
+        # radix-sort histogram + scan + one pass per 8 key bits, gather
+        "gpu_launches": args.steps * kernels_per_step + args.steps +
+                        resorts * (4 + (int(np.ceil(np.log2(max(int(np.prod(p.ncell)), 2)))) + 7) // 8),
         "clocks": clocks,
         "wall_s": wall,
         "kernel_ms_per_step": [float(x) for x in kms.mean(axis=0)],
