@@ -273,7 +273,7 @@ __device__ __forceinline__ void adj_deposit_body(const DevParams& P, const DevSt
         for (int c = 0; c < NS; c++) fN[c] = f[c * S.cap + p] * S.Nn[c / NH][p];
     }
     tile_deposit_block<NF, SWt, double>(P, mesh, active, st, fN, vx, vy, vz,
-                                        [](double a, int) -> double { return a; });
+                                        [](double a, int) -> double { return a; }, true);
 }
 
 struct AdjStagePtrs {
@@ -451,7 +451,7 @@ __device__ __forceinline__ void adj_fwd_stage4_next_body(const DevParams& P, con
     }
     if (mesh_next)
         tile_deposit_block<NF, SWt, double>(P, mesh_next, active, st, fN, vx, vy, vz,
-                                            [](double a, int) -> double { return a; });
+                                            [](double a, int) -> double { return a; }, true);
 }
 
 template <int NF, int WX, int WY, int WZ>

@@ -56,6 +56,8 @@ void emu::make_devparams(const emu_params& p, DevParams& P)
         P.dxi[d] = 1.0 / dx[d];
     }
     P.ncells = (long long)p.ncell[0] * p.ncell[1] * p.ncell[2];
+    P.key_bits = 1;
+    while ((1ll << P.key_bits) <= P.ncells) P.key_bits++;
     const double inv_cell_volume = P.dxi[0] * P.dxi[1] * P.dxi[2];
     P.cell_volume = dx[0] * dx[1] * dx[2];
     P.GF = emu_host::gf();

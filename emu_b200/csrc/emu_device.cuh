@@ -58,6 +58,7 @@ struct DevParams {
     int w[3];          // stencil width per dimension (order+1, order 0 for 1-cell dims)
     int ord[3];        // shape order per dimension
     long long ncells;
+    int key_bits;      // bits of a stencil key in [0, ncells]
     double L[3];       // domain length (periodic, [0,L))
     double dxi[3];     // inverse cell size
     double sqrt2GF_inv_vol;   // sqrt(2)*GF*inv_cell_volume (Evolve.cpp:167 + fill)
@@ -346,20 +347,80 @@ __device__ __forceinline__ void load_weights(const R* r, R (&w)[SP])
     }
 }
 
+// Run accumulators of the tile deposit: S stencil-cell sums of one mesh
+// component.  FP32 sums use Blackwell's packed FP32x2 FMA (two cells per
+// instruction; SP pads S to an even count with zero weights).
+__device__ __forceinline__ unsigned long long f32x2(float a, float b)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+template <class R, int S, int SP>
+struct RunAcc {
+    R a[S];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < S; k++) a[k] = (R)0;
+    }
+    __device__ __forceinline__ void add(const R (&w)[SP], R q)
+    {
+#pragma unroll
+        for (int k = 0; k < S; k++) a[k] += w[k] * q;
+    }
+    __device__ __forceinline__ R get(int k) const { return a[k]; }
+};
+
+template <int S, int SP>
+struct RunAcc<float, S, SP> {
+    static constexpr int NP = (S + 1) / 2;
+    static_assert(2 * NP <= SP, "padded weights");
+    unsigned long long a[NP];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < NP; k++) a[k] = 0ull;
+    }
+    __device__ __forceinline__ void add(const float (&w)[SP], float q)
+    {
+        const unsigned long long qq = f32x2(q, q);
+#pragma unroll
+        for (int k = 0; k < NP; k++)
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(a[k]) : "l"(f32x2(w[2 * k], w[2 * k + 1])), "l"(qq));
+    }
+    __device__ __forceinline__ float get(int k) const
+    {
+        float lo, hi;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a[k / 2]));
+        return (k & 1) ? hi : lo;
+    }
+};
+
+// Phase B of the tile deposit: thread q owns mesh component q of every
+// stencil cell; it walks its stream of records (contiguous, in key order
+// through sidx when given), sums each run
+// of equal stencil keys in registers and adds the run total with one atomic
+// per (cell, component).  Inside a run, aligned groups of four records with
+// the run's key are summed without per-record key tests.
 template <int NF, int BLOCK, class SWt, class R, class T, class Conv>
-__device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const R* srec, int ntile,
-                                             Conv conv)
+__device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const int* sidx,
+                                             const R* srec, int ntile, Conv conv)
 {
     using TR = TileRec<NF, SWt, R>;
     constexpr int NH = NF * NF, NS = 2 * NH, ND = 8 * NH, RW = TR::RW, SP = TR::SP;
     constexpr int NDP = (ND + 31) / 32 * 32;
     constexpr int NSTREAM = BLOCK / NDP > 0 ? BLOCK / NDP : 1;
+    constexpr int CH = BLOCK / NSTREAM;
     constexpr int SX = SWt::MX, SY = SWt::MY, SZ = SWt::MZ;
     const int q = threadIdx.x % NDP;
     const int stream = threadIdx.x / NDP;
     if (stream >= NSTREAM || q >= ND) return;   // no block-wide barrier follows inside
     const int dir = q / (2 * NH), sp = (q / NH) & 1, e = q % NH;
-    R acc[SZ * SY * SX];
+    const int boff = SP + sp * NH + e;               // f N of this component
+    const int voff = SP + NS + (dir > 0 ? dir - 1 : 0);
+    RunAcc<R, SZ * SY * SX, SP> acc;
     auto flush = [&](int key) {
         const int bx = key % P.n[0];
         const int by = (key / P.n[0]) % P.n[1];
@@ -371,27 +432,44 @@ __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const 
 #pragma unroll
                 for (int ii = 0; ii < SX; ii++) {
                     if (!SWt::on(P, ii, jj, kk)) continue;
-                    const T v = conv(acc[(kk * SY + jj) * SX + ii], sp);
+                    const T v = conv(acc.get((kk * SY + jj) * SX + ii), sp);
                     if (v != (T)0) atomic_add_mesh(&mesh[cell_of(P, bx, by, bz, ii, jj, kk) * ND + q], v);
                 }
     };
+    auto add_one = [&](int i) {
+        const R* r = srec + (sidx ? sidx[i] : i) * RW;
+        const R b = r[boff];
+        const R qv = dir == 0 ? b : b * r[voff];
+        R w[SP];
+        load_weights<R, SP>(r, w);
+        acc.add(w, qv);
+    };
+    const int i1 = min((stream + 1) * CH, ntile);
     int cur = -1;
-    for (int i = stream; i < ntile; i += NSTREAM) {
+    acc.zero();
+    // FP64 27-cell runs keep the plain loop (their accumulators and weights
+    // already fill the registers)
+    constexpr bool QUAD = sizeof(R) == 4 || SX * SY * SZ <= 4;
+    for (int i = stream * CH; i < i1;) {
+        if (QUAD && (i & 3) == 0 && i + 4 <= i1 && cur >= 0) {
+            const int4 k4 = *reinterpret_cast<const int4*>(skey + i);
+            if (k4.x == cur && k4.y == cur && k4.z == cur && k4.w == cur) {
+                // the compiler hoists the four records' loads as far as the
+                // registers allow (all four for 1D stencils)
+#pragma unroll
+                for (int u = 0; u < 4; u++) add_one(i + u);
+                i += 4;
+                continue;
+            }
+        }
         const int key = skey[i];
         if (key != cur) {
             if (cur >= 0) flush(cur);
-#pragma unroll
-            for (int k = 0; k < SZ * SY * SX; k++) acc[k] = (R)0;
+            acc.zero();
             cur = key;
         }
-        if (key < 0) continue;
-        const R* r = srec + i * RW;
-        const R b = r[SP + sp * NH + e];
-        const R qv = dir == 0 ? b : b * r[SP + NS + dir - 1];
-        R w[SP];
-        load_weights<R, SP>(r, w);
-#pragma unroll
-        for (int k = 0; k < SZ * SY * SX; k++) acc[k] += w[k] * qv;
+        if (key >= 0) add_one(i);
+        i++;
     }
     if (cur >= 0) flush(cur);
 }

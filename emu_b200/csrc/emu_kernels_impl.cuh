@@ -20,6 +20,8 @@
 #pragma once
 #include "emu_kernels.cuh"
 
+#include <cub/block/block_radix_sort.cuh>
+
 #include <climits>
 #include <cstdio>
 
@@ -306,7 +308,7 @@ __device__ __forceinline__ unsigned reduce_blocks(const DevParams& P)
 template <int NF, class SWt, class R>
 __host__ __device__ constexpr int tile_smem_bytes()
 {
-    return kBlock * 4 + kBlock * TileRec<NF, SWt, R>::RW * (int)sizeof(R);
+    return kBlock * 8 + kBlock * TileRec<NF, SWt, R>::RW * (int)sizeof(R);
 }
 
 // int64 fixed-point conversion of a run total (mixed path)
@@ -318,16 +320,36 @@ struct QuantConv {
     }
 };
 
+// sort_keys: the CTA's particles are not in stencil order (the deposit of
+// moved particles at the end of a step): the 128 keys are radix-sorted in
+// shared memory first, so that each stencil forms one run
 template <int NF, class SWt, class R, class T, class Conv>
 __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
-                                                   const R* fN, R vx, R vy, R vz, Conv conv)
+                                                   const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false)
 {
+    using Sort = cub::BlockRadixSort<unsigned, kBlock, 1, int>;
+    static_assert(sizeof(typename Sort::TempStorage) <= kBlock * TileRec<NF, SWt, R>::RW * sizeof(R),
+                  "sort scratch aliases the record area");
     extern __shared__ __align__(16) unsigned char tile_smem[];
     int* skey = reinterpret_cast<int*>(tile_smem);
-    R* srec = reinterpret_cast<R*>(tile_smem + kBlock * 4);
-    tile_record<NF, SWt, R>(srec, skey, threadIdx.x, active ? stencil_key(P, st.b) : -1, fN, vx, vy, vz, st);
+    int* srank = skey + kBlock;
+    R* srec = reinterpret_cast<R*>(tile_smem + kBlock * 8);
+    const int key = active ? stencil_key(P, st.b) : -1;
+    int slot = threadIdx.x;
+    if (sort_keys) {
+        // sort the keys (scratch in the record area, not yet written), then
+        // every thread writes its record at its key's rank
+        auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
+        unsigned k[1] = {key >= 0 ? (unsigned)key : (unsigned)P.ncells};   // inactive slots last
+        int v[1] = {(int)threadIdx.x};
+        Sort(tmp).Sort(k, v, 0, P.key_bits);
+        srank[v[0]] = threadIdx.x;
+        __syncthreads();
+        slot = srank[threadIdx.x];
+    }
+    tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
     __syncthreads();
-    tile_deposit<NF, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
+    tile_deposit<NF, kBlock, SWt, R, T>(P, mesh, skey, nullptr, srec, kBlock, conv);
 }
 
 // ===========================================================================
@@ -452,7 +474,7 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
         }
     }
     tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
-                                        [](double a, int) -> double { return a; });
+                                        [](double a, int) -> double { return a; }, s == 4);
 }
 
 template <int NF, int WX, int WY, int WZ>
@@ -552,7 +574,7 @@ __global__ void __launch_bounds__(kBlock) k_deposit(DevParams P, DevState S, con
         }
     }
     tile_deposit_block<NF, SWt, double>(P, mesh, active, st, fN, vx, vy, vz,
-                                        [](double a, int) -> double { return a; });
+                                        [](double a, int) -> double { return a; }, true);
 }
 
 template <int NF, int WX, int WY, int WZ>
@@ -698,7 +720,7 @@ __global__ void __launch_bounds__(kBlock) k_deposit_q(DevParams P, DevState S, c
             fN[NH + e] = (float)f[(NH + e) * S.cap + p] * N1;
         }
     }
-    tile_deposit_block<NF, SWt, float>(P, mesh, active, st, fN, vx, vy, vz, QuantConv{P});
+    tile_deposit_block<NF, SWt, float>(P, mesh, active, st, fN, vx, vy, vz, QuantConv{P}, true);
 }
 
 // FP32 self-interaction potential from the finalized mesh: H_SI,e (nu); the
@@ -881,7 +903,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
             make_stencil<float>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P});
+    tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4);
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
 }
 
