@@ -309,29 +309,56 @@ def run_emu(args):
         with open(tpath) as f:
             traffic = json.load(f).get("bytes_per_launch")
 
-    # end to end through the C ABI with host buffers: upload the state from
-    # pinned memory, one device step, download the state
+    # end to end through the C ABI with host buffers: every step uploads its
+    # particles from pinned host memory, runs one device step and downloads
+    # the state.  One GPU: `--e2e-pipes` independent batches, each with its
+    # own context, stream and host thread, so that one batch's copies overlap
+    # another's compute (PCIe copies in both directions run concurrently).
     e2e = None
     if not args.no_e2e:
-        pin_in = torch.from_numpy(recs).pin_memory()
-        pin_out = torch.empty_like(pin_in).pin_memory()
+        import threading
+        pipes = args.e2e_pipes if ws == 1 else 1
         ne = min(args.steps, args.e2e_steps)
+        lanes = []
+        for k in range(pipes):
+            if k == 0:
+                c, s_ = ctx, stream
+            else:
+                s_ = torch.cuda.Stream()
+                c = api.Context(p)
+                c.set_stream(s_.cuda_stream)
+            lanes.append((c, torch.from_numpy(recs).pin_memory(), torch.empty_like(torch.from_numpy(recs)).pin_memory()))
+
+        def lane(c, pin_in, pin_out, count):
+            for _ in range(count):
+                c.load_particles_ptr(pin_in.data_ptr(), n)
+                c.evolve_begin(0.0, float("inf"), 1)
+                c.evolve_steps(1)
+                c.get_particles_ptr(pin_out.data_ptr(), n)
+
+        for c, pi, po in lanes:      # untimed: graphs and buffers of every lane
+            lane(c, pi, po, 2)
         torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        threads = [threading.Thread(target=lane, args=(c, pi, po, ne)) for c, pi, po in lanes]
         e0 = time.perf_counter()
-        for _ in range(ne):
-            ctx.load_particles_ptr(pin_in.data_ptr(), n)
-            ctx.evolve_begin(0.0, float("inf"), 1)
-            ctx.evolve_steps(1)
-            ctx.get_particles_ptr(pin_out.data_ptr(), n)
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
         el = time.perf_counter() - e0
         t = torch.tensor([el], dtype=torch.float64, device="cuda")
         if ws > 1:
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        for c, _, _ in lanes[1:]:
+            c.close()
         bytes_rec = n * api.nreal(nf) * 8
-        e2e = {"value": n * ne * ws / float(t.item()), "unit": "particle-steps/s",
-               "h2d_bytes_per_step": bytes_rec, "d2h_bytes_per_step": bytes_rec,
-               "note": "per step: emu_load_particles from pinned host memory, emu_evolve_begin "
-                       "(deposit + compute_dt), one device step, emu_get_particles to pinned host memory"}
+        e2e = {"value": n * ne * pipes * ws / float(t.item()), "unit": "particle-steps/s",
+               "h2d_bytes_per_step": bytes_rec, "d2h_bytes_per_step": bytes_rec, "batches_in_flight": pipes,
+               "note": "per step of a batch: emu_load_particles from pinned host memory, emu_evolve_begin "
+                       "(deposit + compute_dt), one device step, emu_get_particles to pinned host memory; "
+                       "%d batches with their own contexts and host threads run concurrently" % pipes}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -440,6 +467,8 @@ def main():
                     help="particle-sharded path even on one GPU (a one-rank communicator)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-pipes", type=int, default=4,
+                    help="batches in flight for the end-to-end figure (one GPU)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
