@@ -291,13 +291,14 @@ def run_emu(args):
     kms = np.array(kms)
     per_pstep = algorithmic_bytes_per_particle_step(nf, mixed)
     coop = kms.shape[1] == 1
+    split = nf == 2 and p.ncell[0] == 1 and p.ncell[1] == 1 and not mixed   # species-split kernels
     if coop:
         # one cooperative kernel per step: the whole step is the launch
-        kernel = "k_rk4_step_coop<%d>" % nf
+        kernel = "k_rk4_step_coop%s<%d>" % ("_split" if split else "", nf)
         stage_ms = float(kms[:, 0].mean())
         bytes_per_launch = per_pstep * n + mesh_bytes_per_step(p, nf)
     else:
-        kernel = "k_rk4_stage%s<%d>" % ("_mixed" if mixed else "", nf)
+        kernel = "k_rk4_stage%s<%d>" % ("_mixed" if mixed else ("_split" if split else ""), nf)
         stage_idx = [1, 3, 5, 7] if mixed else [0, 1, 2, 3]
         stage_ms = float(kms[:, stage_idx].mean())
         bytes_per_launch = (per_pstep * n + mesh_bytes_per_step(p, nf)) / 4.0
@@ -305,9 +306,13 @@ def run_emu(args):
     achieved = bytes_per_launch / (stage_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (args.workload, "mixed" if mixed else "fp64"))
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and args.cells is None:
         with open(tpath) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+            tj = json.load(f)
+        # DRAM bytes per launch of this kernel from the ncu capture (scaled
+        # from the captured case's particle count when it was a smaller one)
+        if tj.get("kernel", "").split("<")[0] == kernel.split("<")[0]:
+            traffic = tj.get("bytes_per_launch")
 
     # end to end through the C ABI with host buffers: every step uploads its
     # particles from pinned host memory, runs one device step and downloads
@@ -460,7 +465,8 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"])
     ap.add_argument("--cells", type=int, default=None, help="smaller case of the workload (cells per side)")
     ap.add_argument("--fused", type=int, default=None, choices=[1, 2],
-                    help="RK4 kernels: 2 one cooperative launch per step when it fits (default), 1 per stage")
+                    help="RK4 kernels: 1 one fused kernel per stage in a CUDA graph (default), 2 one "
+                         "cooperative launch per step when it fits")
     ap.add_argument("--resort", type=int, default=None,
                     help="steps between on-device cell re-sorts (0 never; default the workload's)")
     ap.add_argument("--sharded", action="store_true",

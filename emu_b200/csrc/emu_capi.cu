@@ -389,6 +389,8 @@ int build_graph(emu_context* ctx)
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     ctx->graph[ctx->cur] = ex;
+    ctx->graph_P[ctx->cur] = ctx->P;
+    ctx->graph_S[ctx->cur] = ctx->S[ctx->cur];
     return EMU_OK;
 }
 
@@ -409,8 +411,17 @@ int emu_ctx::step_device(emu_context* ctx)
                                                   emu::DT_ADVANCE, ctx->stream);
         if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
     } else {
-        if (!ctx->graph[ctx->cur] && (r = build_graph(ctx))) return r;
-        CU(cudaGraphLaunch(ctx->graph[ctx->cur], ctx->stream));
+        const int c = ctx->cur;
+        // the graph holds its kernels' arguments by value: re-capture when
+        // the parameters or the particle arrays changed since (a reload of
+        // a different set); a reload of an equal set reuses it
+        if (ctx->graph[c] && (std::memcmp(&ctx->graph_P[c], &ctx->P, sizeof(DevParams)) != 0 ||
+                              std::memcmp(&ctx->graph_S[c], &ctx->S[c], sizeof(DevState)) != 0)) {
+            cudaGraphExecDestroy(ctx->graph[c]);
+            ctx->graph[c] = nullptr;
+        }
+        if (!ctx->graph[c] && (r = build_graph(ctx))) return r;
+        CU(cudaGraphLaunch(ctx->graph[c], ctx->stream));
     }
     ctx->cur_mesh = ctx->mixed ? 1 : 3;
     return EMU_OK;
@@ -588,8 +599,8 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     emu::launch_pack(ctx->nf, ctx->P, ctx->aos, ctx->idx2, n, S, ctx->stream);
     if (ctx->mixed) emu::launch_mixed_shadow(ctx->nf, S, ctx->stream);
     if ((r = check_launch(ctx, "pack"))) return r;
-    free_graphs(ctx);   // kernel arguments (P, S) changed
-    // fused == 2 (default): one cooperative launch per step when the grid fits
+    // (step graphs re-capture themselves when P or S differ from their capture)
+    // fused == 2: one cooperative launch per step when the grid fits
     // (a sharded run reduces every deposit between stages: per-stage kernels)
     ctx->coop = !ctx->mixed && !ctx->comm && ctx->prm.fused == 2 && rk4_fused(ctx) &&
                 emu::coop_step_fits(ctx->nf, ctx->P, n);

@@ -43,6 +43,8 @@ struct emu_context {
     bool fused_ready = false;
     bool loaded = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    DevParams graph_P[2];               // kernel arguments each graph was captured with
+    DevState graph_S[2];
     int steps_since_sort = 0;
     bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
     emu_adjoint* adj = nullptr;         // allocated by the first adjoint call

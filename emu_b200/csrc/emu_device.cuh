@@ -404,7 +404,7 @@ struct RunAcc<float, S, SP> {
 // of equal stencil keys in registers and adds the run total with one atomic
 // per (cell, component).  Inside a run, aligned groups of four records with
 // the run's key are summed without per-record key tests.
-template <int NF, int BLOCK, class SWt, class R, class T, class Conv>
+template <int NF, int BLOCK, int NTILE, class SWt, class R, class T, class Conv>
 __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const int* sidx,
                                              const R* srec, int ntile, Conv conv)
 {
@@ -412,7 +412,8 @@ __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const 
     constexpr int NH = NF * NF, NS = 2 * NH, ND = 8 * NH, RW = TR::RW, SP = TR::SP;
     constexpr int NDP = (ND + 31) / 32 * 32;
     constexpr int NSTREAM = BLOCK / NDP > 0 ? BLOCK / NDP : 1;
-    constexpr int CH = BLOCK / NSTREAM;
+    constexpr int CH = NTILE / NSTREAM;   // records per stream (a multiple of 4)
+    static_assert(CH % 4 == 0, "stream chunks hold whole groups of four records");
     constexpr int SX = SWt::MX, SY = SWt::MY, SZ = SWt::MZ;
     const int q = threadIdx.x % NDP;
     const int stream = threadIdx.x / NDP;

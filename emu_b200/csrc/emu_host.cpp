@@ -471,7 +471,7 @@ void emu_params_default(emu_params* p)
     p->ndirections = 0;
     p->seed = 0;
     p->resort_interval = -1;
-    p->fused = 2;
+    p->fused = 1;
 }
 
 int emu_parse_inputs(const char* path, int n_overrides, const char* const* overrides, emu_params* out,
@@ -514,7 +514,7 @@ int emu_parse_inputs(const char* path, int n_overrides, const char* const* overr
     p.ndirections = g.i_or("emu.ndirections", 0);
     p.seed = (uint64_t)g.d_or("emu.seed", 0);
     p.resort_interval = g.i_or("emu.resort_interval", -1);
-    p.fused = g.i_or("emu.fused", 2);
+    p.fused = g.i_or("emu.fused", 1);
     // integrator keys read by the AMReX TimeIntegrator
     p.integration_type = g.i("integration.type");
     if (p.integration_type == 1) p.rk_type = g.i("integration.rk.type");

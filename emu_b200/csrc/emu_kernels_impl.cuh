@@ -349,7 +349,59 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
     }
     tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
     __syncthreads();
-    tile_deposit<NF, kBlock, SWt, R, T>(P, mesh, skey, nullptr, srec, kBlock, conv);
+    tile_deposit<NF, kBlock, kBlock, SWt, R, T>(P, mesh, skey, nullptr, srec, kBlock, conv);
+}
+
+// The same for a species-split CTA (kBlock particles, 2 kBlock threads:
+// thread t works on species t / kBlock of particle t % kBlock).  Both threads
+// of a particle write their species' f N into its record; the species-0
+// thread writes the key, weights and velocity.
+template <int NF, class SWt, class R, class T, class Conv>
+__device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* mesh, bool active,
+                                                         const Stencil<R>& st, int sp, const R* fNs, R vx, R vy, R vz,
+                                                         Conv conv, bool sort_keys)
+{
+    using TR = TileRec<NF, SWt, R>;
+    constexpr int NT = 2 * kBlock, NH = NF * NF, RW = TR::RW, SP = TR::SP;
+    using Sort = cub::BlockRadixSort<unsigned, NT, 1, int>;
+    static_assert(sizeof(typename Sort::TempStorage) <= kBlock * RW * sizeof(R), "sort scratch aliases the records");
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    int* skey = reinterpret_cast<int*>(tile_smem);
+    int* srank = skey + kBlock;
+    R* srec = reinterpret_cast<R*>(tile_smem + kBlock * 8);
+    const int pl = threadIdx.x % kBlock;
+    const int key = active ? stencil_key(P, st.b) : -1;
+    int slot = pl;
+    if (sort_keys) {
+        // species-1 threads sort behind every real key (ncells + 1)
+        auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
+        unsigned k[1] = {sp ? (unsigned)P.ncells + 1u : (key >= 0 ? (unsigned)key : (unsigned)P.ncells)};
+        int v[1] = {(int)threadIdx.x};
+        Sort(tmp).Sort(k, v, 0, P.key_bits + 1);
+        if (threadIdx.x < kBlock) srank[v[0]] = threadIdx.x;
+        __syncthreads();
+        slot = srank[pl];
+    }
+    R* r = srec + slot * RW;
+    if (sp == 0) {
+        skey[slot] = key;
+#pragma unroll
+        for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+            for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+                for (int ii = 0; ii < SWt::MX; ii++)
+                    r[(kk * SWt::MY + jj) * SWt::MX + ii] = (st.wx[ii] * st.wy[jj]) * st.wz[kk];
+#pragma unroll
+        for (int k = TR::S; k < SP; k++) r[k] = (R)0;
+        r[SP + TR::NS + 0] = vx;
+        r[SP + TR::NS + 1] = vy;
+        r[SP + TR::NS + 2] = vz;
+    }
+#pragma unroll
+    for (int e = 0; e < NH; e++) r[SP + sp * NH + e] = fNs[e];
+    __syncthreads();
+    tile_deposit<NF, NT, kBlock, SWt, R, T>(P, mesh, skey, nullptr, srec, kBlock, conv);
 }
 
 // ===========================================================================
@@ -477,6 +529,141 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
                                         [](double a, int) -> double { return a; }, s == 4);
 }
 
+// FP64 potential of one species (potential_fp64 restricted to species sp)
+template <int NF, class SWt>
+__device__ __forceinline__ void potential_fp64_sp(const DevParams& P, const double* __restrict__ mesh,
+                                                  const Stencil<double>& st, double vx, double vy, double vz,
+                                                  double vscale, int sp, double* V)
+{
+    using H = Herm<NF>;
+    constexpr int NH = NF * NF, ND = 8 * NH;
+#pragma unroll
+    for (int e = 0; e < NH; e++) V[e] = P.M2[sp][e] * vscale;
+    STENCIL_LOOP(SWt, {
+        const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
+        const double* __restrict__ m = mesh + cell * ND;
+        const double coef = ((P.sqrt2GF_inv_vol * st.wx[ii]) * st.wy[jj]) * st.wz[kk];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            const double SI = __ldg(m + e) - __ldg(m + 2 * NH + e) * vx - __ldg(m + 4 * NH + e) * vy -
+                              __ldg(m + 6 * NH + e) * vz;
+            const double Sb = __ldg(m + NH + e) - __ldg(m + 3 * NH + e) * vx - __ldg(m + 5 * NH + e) * vy -
+                              __ldg(m + 7 * NH + e) * vz;
+            double inside = H::is_im(e) ? SI + Sb : SI - Sb;
+            if (e == 0) inside = inside + P.matter;
+            const double t = coef * inside;
+            if (sp == 0 || H::is_im(e)) V[e] += t; else V[e] -= t;
+        }
+    })
+}
+
+// Species-split FP64 RK4 stage (1D stencils): thread t advances species
+// t / kBlock of particle t % kBlock; same arithmetic as rk4_stage_body.
+template <int NF, class SWt>
+__device__ __forceinline__ void rk4_stage_body_split(const DevParams& P, const DevState& S, int s,
+                                                     const double* __restrict__ mesh_in, double* __restrict__ mesh_out,
+                                                     double* mesh_zero, long long nzero, StepCtl* ctl, double dt)
+{
+    constexpr int NH = NF * NF;
+    zero_slice(mesh_zero, nzero);
+    const int sp = threadIdx.x / kBlock;
+    const long long p = (long long)blockIdx.x * kBlock + threadIdx.x % kBlock;
+    const bool active = p < S.n;
+    const long long cap = S.cap;
+    Stencil<double> st{};
+    double fN[NH] = {};
+    double vx = 0, vy = 0, vz = 0;
+    if (active) {
+        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
+        vx = S.vhat[0][p];
+        vy = S.vhat[1][p];
+        vz = S.vhat[2][p];
+        const double* __restrict__ fin = s == 1 ? S.f0 : S.fs;
+        const double vsc = S.vscale[p];
+        const double Ns = S.Nn[sp][p];
+        const double Ls = s == 4 ? S.Ll[sp][p] : 0.0;
+        const double t_in = (s == 4 && sp == 0) ? S.time[p] : 0.0;
+        double f[NH], y0[NH], a0[NH];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            const long long o = (sp * NH + e) * cap + p;
+            f[e] = fin[o];
+            y0[e] = s > 1 ? S.f0[o] : 0.0;
+            a0[e] = s > 1 ? S.acc[o] : 0.0;
+        }
+        make_stencil<double>(P, x, y, z, st);
+        double V[NH], K[NH];
+        potential_fp64_sp<NF, SWt>(P, mesh_in, st, vx, vy, vz, vsc, sp, V);
+        commutator<NF, double>(V, f, K, P.inv_hbar);
+        const double bw = dt * kRK4B[s - 1];
+        const double aw = s < 4 ? dt * kRK4A[s] : 0.0;
+        double* fn = f;
+        int stt = 0;
+        if (s < 4) {
+#pragma unroll
+            for (int e = 0; e < NH; e++) {
+                const long long o = (sp * NH + e) * cap + p;
+                const double yy = (s == 1) ? f[e] : y0[e];
+                const double aa = (s == 1) ? yy : a0[e];
+                S.acc[o] = __dadd_rn(__dmul_rn(bw, K[e]), aa);
+                fn[e] = __dadd_rn(__dmul_rn(aw, K[e]), yy);
+                S.fs[o] = fn[e];
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < NH; e++) fn[e] = __dadd_rn(__dmul_rn(bw, K[e]), a0[e]);
+            stt = renormalize<NF>(fn, Ls, P.maxError);
+#pragma unroll
+            for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
+        }
+#pragma unroll
+        for (int e = 0; e < NH; e++) fN[e] = fn[e] * Ns;
+        if (s == 4) {
+            double xn[3] = {x, y, z};
+            const double kxv[3] = {vx * kC, vy * kC, vz * kC};
+            double tn = t_in;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const double w = dt * kRK4B[i];
+#pragma unroll
+                for (int d = 0; d < 3; d++) xn[d] = __dadd_rn(__dmul_rn(w, kxv[d]), xn[d]);
+                tn = __dadd_rn(w, tn);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) xn[d] = wrap_coord(xn[d], P.L[d]);
+            if (sp == 0) {
+#pragma unroll
+                for (int d = 0; d < 3; d++) S.pos[d][p] = xn[d];
+                S.time[p] = tn;
+            }
+            report_bad(ctl, stt, S.id[p]);
+            make_stencil<double>(P, xn[0], xn[1], xn[2], st);
+        }
+    }
+    tile_deposit_block_split<NF, SWt, double>(P, mesh_out, active, st, sp, fN, vx, vy, vz,
+                                              [](double a, int) -> double { return a; }, s == 4);
+}
+
+// Two flavors, 1D stencils: species-split kernels (2 kBlock threads per
+// CTA).  Three flavors keep one thread per particle: the split duplicates a
+// 72-component mesh gather per thread and exceeds the register budget.
+template <int NF, int WX, int WY>
+constexpr bool kSplit = NF == 2 && WX == 1 && WY == 1;
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(2 * kBlock, 2) k_rk4_stage_split(DevParams P, DevState S, int s,
+                                                                  const double* __restrict__ mesh_in,
+                                                                  double* __restrict__ mesh_out, double* mesh_zero,
+                                                                  long long nzero, StepCtl* ctl, int dt_mode)
+{
+    const int done = ctl->done;
+    const double dt = ctl->dt;
+    if (done) return;
+    if (s == 1) record_dt(ctl, dt);
+    rk4_stage_body_split<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt);
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+}
+
 template <int NF, int WX, int WY, int WZ>
 __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S, int s, const double* __restrict__ mesh_in,
                                                       double* __restrict__ mesh_out, double* mesh_zero, long long nzero,
@@ -537,13 +724,33 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_step_coop(DevParams P, DevSta
     const double dt = ctl->dt;
     if (done) return;
     record_dt(ctl, dt);
-    rk4_stage_body<NF, SWt>(P, S, 1, m0, m1, m2, nmesh, ctl, dt);
-    grid_barrier(ctl);
-    rk4_stage_body<NF, SWt>(P, S, 2, m1, m2, m3, nmesh, ctl, dt);
-    grid_barrier(ctl);
-    rk4_stage_body<NF, SWt>(P, S, 3, m2, m3, m0, nmesh, ctl, dt);
-    grid_barrier(ctl);
-    rk4_stage_body<NF, SWt>(P, S, 4, m3, m0, m1, nmesh, ctl, dt);
+    double* const m[4] = {m0, m1, m2, m3};
+#pragma unroll 1
+    for (int s = 1; s <= 4; s++) {
+        rk4_stage_body<NF, SWt>(P, S, s, m[s - 1], m[s % 4], m[(s + 1) % 4], nmesh, ctl, dt);
+        if (s < 4) grid_barrier(ctl);
+    }
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, m3, ctl, DT_ADVANCE, reduce_blocks(P));
+}
+
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(2 * kBlock, 2) k_rk4_step_coop_split(DevParams P, DevState S, double* m0, double* m1,
+                                                                      double* m2, double* m3, long long nmesh,
+                                                                      StepCtl* ctl, int dt_mode)
+{
+    using SWt = SW<WX, WY, WZ>;
+    const int done = ctl->done;
+    const double dt = ctl->dt;
+    if (done) return;
+    record_dt(ctl, dt);
+    // one copy of the stage body (a runtime stage loop): every instruction
+    // of the step runs only a few times, so code size costs fetch stalls
+    double* const m[4] = {m0, m1, m2, m3};
+#pragma unroll 1
+    for (int s = 1; s <= 4; s++) {
+        rk4_stage_body_split<NF, SWt>(P, S, s, m[s - 1], m[s % 4], m[(s + 1) % 4], nmesh, ctl, dt);
+        if (s < 4) grid_barrier(ctl);
+    }
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, m3, ctl, DT_ADVANCE, reduce_blocks(P));
 }
 
@@ -1119,9 +1326,15 @@ void launch_rk4_stage_t(const DevParams& P, const DevState& S, int s, const doub
 {
     EMU_W_DISPATCH(P, {
         constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
-        smem_optin(k_rk4_stage<NF, WXv, WYv, WZv>, bytes);
-        k_rk4_stage<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, s, mesh_in, mesh_out, mesh_zero,
-                                                                            nzero, ctl, dt_mode);
+        if constexpr (kSplit<NF, WXv, WYv>) {
+            smem_optin(k_rk4_stage_split<NF, WXv, WYv, WZv>, bytes);
+            k_rk4_stage_split<NF, WXv, WYv, WZv><<<grid_for(S.n), 2 * kBlock, bytes, st>>>(
+                P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt_mode);
+        } else {
+            smem_optin(k_rk4_stage<NF, WXv, WYv, WZv>, bytes);
+            k_rk4_stage<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, s, mesh_in, mesh_out,
+                                                                                mesh_zero, nzero, ctl, dt_mode);
+        }
     });
 }
 
@@ -1131,12 +1344,14 @@ bool coop_step_fits_t(const DevParams& P, long long n)
     bool ok = false;
     EMU_W_DISPATCH(P, {
         constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
-        auto kern = k_rk4_step_coop<NF, WXv, WYv, WZv>;
+        constexpr bool split = kSplit<NF, WXv, WYv>;
+        auto kern = split ? k_rk4_step_coop_split<NF, WXv, WYv, WZv> : k_rk4_step_coop<NF, WXv, WYv, WZv>;
         smem_optin(kern, bytes);
         int per_sm = 0, dev = 0, nsm = 0;
         if (cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, bytes) == cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, split ? 2 * kBlock : kBlock, bytes) ==
+                cudaSuccess)
             ok = (long long)per_sm * nsm >= (long long)grid_for(n);
     });
     cudaGetLastError();
@@ -1150,7 +1365,8 @@ cudaError_t launch_rk4_step_coop_t(const DevParams& P, const DevState& S, double
     cudaError_t err = cudaSuccess;
     EMU_W_DISPATCH(P, {
         constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
-        auto kern = k_rk4_step_coop<NF, WXv, WYv, WZv>;
+        constexpr bool split = kSplit<NF, WXv, WYv>;
+        auto kern = split ? k_rk4_step_coop_split<NF, WXv, WYv, WZv> : k_rk4_step_coop<NF, WXv, WYv, WZv>;
         smem_optin(kern, bytes);
         DevParams Pc = P;
         DevState Sc = S;
@@ -1159,7 +1375,8 @@ cudaError_t launch_rk4_step_coop_t(const DevParams& P, const DevState& S, double
         StepCtl* c = ctl;
         int mode = dt_mode;
         void* args[] = {&Pc, &Sc, &m0, &m1, &m2, &m3, &nm, &c, &mode};
-        err = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid_for(S.n)), dim3(kBlock), args, bytes, st);
+        err = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid_for(S.n)), dim3(split ? 2 * kBlock : kBlock),
+                                          args, bytes, st);
     });
     return err;
 }

@@ -105,9 +105,9 @@ typedef struct emu_params {
     int resort_interval;     /* steps between on-device cell re-sorts (0 = never,
                                 < 0 = automatic: every step for 3D stencils,
                                 every 4 steps otherwise; default -1) */
-    int fused;               /* RK4 kernels: 2 (default) one cooperative launch per step when
-                                the grid fits on the GPU at once (FP64), else as 1;
-                                1: one fused kernel per stage; 0: unfused stages */
+    int fused;               /* RK4 kernels: 1 (default) one fused kernel per stage, a CUDA
+                                graph per step; 2: one cooperative launch per step when the
+                                grid fits on the GPU at once (FP64), else as 1; 0: unfused */
 } emu_params;
 
 /* summary of a device-resident run (emu_evolve) */
