@@ -114,7 +114,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -177,7 +177,9 @@ def run_reference(args):
     ws, rank, local = dist_setup(args)
     if rank != 0:
         return
-    p, desc = workload(args.workload, args.precision, args.cells, args.fused, args.resort)
+    # the emu arm's configuration (with N ranks: N times the directions)
+    p, desc = workload(args.workload, args.precision, args.cells, args.fused, args.resort,
+                       ws if args.workload != "c4" else 1)
     recs = api.init_particles(p)
     nthreads = os.cpu_count() or 1
     from oracle.oracle import Oracle, RefHarness, have_ref
@@ -458,7 +460,7 @@ def run_adjoint(ctx, recs, p, stream, fwd_ms_per_step, interval=25):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000, help="timed steps (C2's run length by default)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="emu", choices=["emu", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
