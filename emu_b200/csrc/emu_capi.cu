@@ -142,10 +142,11 @@ void assign_transient(DevState& S, void* block, int NS, bool mixed, long long ca
 void free_graphs(emu_context* c)
 {
     for (int i = 0; i < 2; i++)
-        if (c->graph[i]) {
-            cudaGraphExecDestroy(c->graph[i]);
-            c->graph[i] = nullptr;
-        }
+        for (int v = 0; v < 2; v++)
+            if (c->graph[i][v]) {
+                cudaGraphExecDestroy(c->graph[i][v]);
+                c->graph[i][v] = nullptr;
+            }
 }
 
 int ensure_capacity(emu_context* ctx, long long n)
@@ -263,20 +264,23 @@ int deposit_current(emu_context* ctx)
 
 // ---- step bodies -----------------------------------------------------------
 // fused FP64 RK4: stage s reads mesh[s-1], deposits mesh[s%4], zeros mesh[(s+1)%4]
-int enqueue_rk4_fp64(emu_context* ctx, cudaStream_t st, bool with_dt)
+// dep4 = false: stage 4 makes no deposit (a re-sort with deposit follows)
+int enqueue_rk4_fp64(emu_context* ctx, cudaStream_t st, bool with_dt, bool dep4 = true)
 {
     const DevState& S = ctx->S[ctx->cur];
     int r;
     for (int s = 1; s <= 4; s++) {
-        emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4], ctx->mesh[(s + 1) % 4],
-                              mesh_elems(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
-        if ((r = emu_ctx::reduce_mesh(ctx, ctx->mesh[s % 4], false, st))) return r;
+        const bool dep = s < 4 || dep4;
+        emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], dep ? ctx->mesh[s % 4] : nullptr,
+                              ctx->mesh[(s + 1) % 4], mesh_elems(ctx), ctx->ctl,
+                              (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
+        if (dep && (r = emu_ctx::reduce_mesh(ctx, ctx->mesh[s % 4], false, st))) return r;
     }
     return check_launch(ctx, "rk4 stage");
 }
 
 // mixed RK4: finalize(q[a] -> g, zero q[b]); stage deposits into q[b]; swap
-int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt)
+int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt, bool dep4 = true)
 {
     const DevState& S = ctx->S[ctx->cur];
     int a = 0;
@@ -285,10 +289,11 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt)
         emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, st);
         // M_4 sits in q[1] (read by stage 4's compute_dt) until the next
         // step's first finalize zeroes it
-        emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->qmesh[1], ctx->ctl,
-                                    (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
+        const bool dep = s < 4 || dep4;
+        emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr, ctx->qmesh[1],
+                                    ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
         int r;
-        if ((r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return r;
+        if (dep && (r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return r;
         a = b;
     }
     return check_launch(ctx, "rk4 mixed stage");
@@ -350,7 +355,10 @@ int step_generic(emu_context* ctx, double dt)
     return EMU_OK;
 }
 
-int resort(emu_context* ctx)
+// deposit: the last stage of the step just taken made no deposit; the
+// gather deposits the new state (cell-sorted) into the next step's first
+// mesh instead (mesh[0] / qmesh[0], zeroed by the step)
+int resort(emu_context* ctx, bool deposit = false)
 {
     DevState& src = ctx->S[ctx->cur];
     DevState& dst = ctx->S[1 - ctx->cur];
@@ -358,7 +366,15 @@ int resort(emu_context* ctx)
     emu::launch_state_keys(ctx->P, src, ctx->keys, ctx->idx, ctx->stream);
     int r;
     if ((r = sort_perm(ctx, src.n))) return r;
-    emu::launch_gather_state(ctx->nf, ctx->mixed, src, dst, ctx->idx2, ctx->stream);
+    if (deposit) {
+        emu::launch_gather_deposit(ctx->nf, ctx->mixed, ctx->P, src, dst, ctx->idx2, ctx->mesh[0], ctx->qmesh[0],
+                                   ctx->stream);
+        if (ctx->mixed) r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[0], true, ctx->stream);
+        else r = emu_ctx::reduce_mesh(ctx, ctx->mesh[0], false, ctx->stream);
+        if (r) return r;
+    } else {
+        emu::launch_gather_state(ctx->nf, ctx->mixed, src, dst, ctx->idx2, ctx->stream);
+    }
     if ((r = check_launch(ctx, "resort"))) return r;
     ctx->cur = 1 - ctx->cur;
     ctx->steps_since_sort = 0;
@@ -368,16 +384,16 @@ int resort(emu_context* ctx)
     return EMU_OK;
 }
 
-int enqueue_step_body(emu_context* ctx, cudaStream_t st)
+int enqueue_step_body(emu_context* ctx, cudaStream_t st, bool dep4)
 {
-    return ctx->mixed ? enqueue_rk4_mixed(ctx, st, true) : enqueue_rk4_fp64(ctx, st, true);
+    return ctx->mixed ? enqueue_rk4_mixed(ctx, st, true, dep4) : enqueue_rk4_fp64(ctx, st, true, dep4);
 }
 
-int build_graph(emu_context* ctx)
+int build_graph(emu_context* ctx, int variant)
 {
     cudaGraph_t g = nullptr;
     CU(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-    int r = enqueue_step_body(ctx, ctx->cap_stream);
+    int r = enqueue_step_body(ctx, ctx->cap_stream, variant == 0);
     cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);
     if (r) {
         if (g) cudaGraphDestroy(g);
@@ -388,9 +404,9 @@ int build_graph(emu_context* ctx)
     e = cudaGraphInstantiate(&ex, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-    ctx->graph[ctx->cur] = ex;
-    ctx->graph_P[ctx->cur] = ctx->P;
-    ctx->graph_S[ctx->cur] = ctx->S[ctx->cur];
+    ctx->graph[ctx->cur][variant] = ex;
+    ctx->graph_P[ctx->cur][variant] = ctx->P;
+    ctx->graph_S[ctx->cur][variant] = ctx->S[ctx->cur];
     return EMU_OK;
 }
 
@@ -402,7 +418,7 @@ bool rk4_fused(const emu_context* ctx)
 }  // namespace
 
 // ===========================================================================
-int emu_ctx::step_device(emu_context* ctx)
+int emu_ctx::step_device(emu_context* ctx, bool last_stage_deposit)
 {
     int r;
     if (ctx->coop) {
@@ -411,17 +427,17 @@ int emu_ctx::step_device(emu_context* ctx)
                                                   emu::DT_ADVANCE, ctx->stream);
         if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
     } else {
-        const int c = ctx->cur;
+        const int c = ctx->cur, v = last_stage_deposit ? 0 : 1;
         // the graph holds its kernels' arguments by value: re-capture when
         // the parameters or the particle arrays changed since (a reload of
         // a different set); a reload of an equal set reuses it
-        if (ctx->graph[c] && (std::memcmp(&ctx->graph_P[c], &ctx->P, sizeof(DevParams)) != 0 ||
-                              std::memcmp(&ctx->graph_S[c], &ctx->S[c], sizeof(DevState)) != 0)) {
-            cudaGraphExecDestroy(ctx->graph[c]);
-            ctx->graph[c] = nullptr;
+        if (ctx->graph[c][v] && (std::memcmp(&ctx->graph_P[c][v], &ctx->P, sizeof(DevParams)) != 0 ||
+                                 std::memcmp(&ctx->graph_S[c][v], &ctx->S[c], sizeof(DevState)) != 0)) {
+            cudaGraphExecDestroy(ctx->graph[c][v]);
+            ctx->graph[c][v] = nullptr;
         }
-        if (!ctx->graph[c] && (r = build_graph(ctx))) return r;
-        CU(cudaGraphLaunch(ctx->graph[c], ctx->stream));
+        if (!ctx->graph[c][v] && (r = build_graph(ctx, v))) return r;
+        CU(cudaGraphLaunch(ctx->graph[c][v], ctx->stream));
     }
     ctx->cur_mesh = ctx->mixed ? 1 : 3;
     return EMU_OK;
@@ -769,9 +785,18 @@ int emu_evolve_steps(emu_context* ctx, int nsteps)
     if (!ctx) return EMU_ERR_ARG;
     int r;
     for (int i = 0; i < nsteps; i++) {
-        if ((r = emu_ctx::step_device(ctx))) return r;
-        if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
-            if ((r = resort(ctx))) return r;
+        // when a re-sort follows this step, its gather makes the deposit of
+        // the new state (in cell order) instead of the last stage
+        const bool resort_next =
+            ctx->prm.resort_interval > 0 && ctx->steps_since_sort + 1 >= ctx->prm.resort_interval;
+        const bool fuse = resort_next && !ctx->coop;
+        if ((r = emu_ctx::step_device(ctx, !fuse))) return r;
+        if (resort_next) {
+            ctx->steps_since_sort++;
+            if ((r = resort(ctx, fuse))) return r;
+        } else if (ctx->prm.resort_interval > 0) {
+            ctx->steps_since_sort++;
+        }
     }
     return EMU_OK;
 }

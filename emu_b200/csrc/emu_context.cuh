@@ -42,9 +42,11 @@ struct emu_context {
     int cur_mesh = 0;
     bool fused_ready = false;
     bool loaded = false;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    DevParams graph_P[2];               // kernel arguments each graph was captured with
-    DevState graph_S[2];
+    // step graphs per particle buffer and variant (0: the last stage deposits
+    // the new state; 1: it does not, the re-sort gather that follows does)
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    DevParams graph_P[2][2];            // kernel arguments each graph was captured with
+    DevState graph_S[2][2];
     int steps_since_sort = 0;
     bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
     emu_adjoint* adj = nullptr;         // allocated by the first adjoint call
@@ -64,8 +66,10 @@ int fail(emu_context* c, int code, const std::string& msg);
 // EMU_ERR_CUDA with what + the pending launch error, if any
 int check_launch(emu_context* ctx, const char* what);
 // one device-resident step of the fused RK4 loop (cooperative kernel or
-// graph), without the periodic re-sort; dt comes from the device control
-int step_device(emu_context* ctx);
+// graph), without the periodic re-sort; dt comes from the device control.
+// last_stage_deposit = false leaves the deposit of the new state to a
+// re-sort with deposit that the caller makes next.
+int step_device(emu_context* ctx, bool last_stage_deposit = true);
 // sum a deposited mesh (FP64, or int64 for the mixed path) over the ranks of
 // the attached communicator, enqueued on st; no-op without one
 int reduce_mesh(emu_context* ctx, void* mesh, bool int64, cudaStream_t st);

@@ -5,6 +5,8 @@ namespace emu {
 template void launch_rk4_stage_t<2>(const DevParams&, const DevState&, int, const double*, double*, double*,
                                     long long, StepCtl*, int, cudaStream_t);
 template void launch_deposit_t<2>(const DevParams&, const DevState&, const double*, double*, cudaStream_t);
+template void launch_gather_deposit_t<2>(bool, const DevParams&, const DevState&, const DevState&, const unsigned*,
+                                         double*, long long*, cudaStream_t);
 template void launch_rhs_t<2>(const DevParams&, const DevState&, const double*, const double*, double*,
                               cudaStream_t);
 template bool coop_step_fits_t<2>(const DevParams&, long long);

@@ -18,6 +18,8 @@ namespace emu {
     extern template void launch_deposit_q_t<NF>(const DevParams&, const DevState&, const double*, long long*,    \
                                                 cudaStream_t);                                                   \
     extern template bool coop_step_fits_t<NF>(const DevParams&, long long);                                      \
+    extern template void launch_gather_deposit_t<NF>(bool, const DevParams&, const DevState&, const DevState&,    \
+                                                     const unsigned*, double*, long long*, cudaStream_t);        \
     extern template cudaError_t launch_rk4_step_coop_t<NF>(const DevParams&, const DevState&, double* const*,    \
                                                            long long, StepCtl*, int, cudaStream_t);
 EMU_EXTERN(2)
@@ -66,6 +68,13 @@ void launch_gather_state(int nf, bool mixed, const DevState& src, const DevState
                          cudaStream_t st)
 {
     EMU_NF_DISPATCH(nf, (k_gather_state<NFv><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, mixed ? 1 : 0)));
+}
+
+void launch_gather_deposit(int nf, bool mixed, const DevParams& P, const DevState& src, const DevState& dst,
+                           const unsigned* perm, double* mesh, long long* qmesh, cudaStream_t st)
+{
+    if (nf == 2) launch_gather_deposit_t<2>(mixed, P, src, dst, perm, mesh, qmesh, st);
+    else launch_gather_deposit_t<3>(mixed, P, src, dst, perm, mesh, qmesh, st);
 }
 
 void launch_deposit(int nf, const DevParams& P, const DevState& S, const double* f, double* mesh, cudaStream_t st)

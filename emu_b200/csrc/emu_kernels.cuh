@@ -109,6 +109,10 @@ void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st);
 void launch_flush(double* buf, long long n, cudaStream_t st);
 // cell re-sort: keys of the current positions, then gather every array
 void launch_state_keys(const DevParams& P, const DevState& S, unsigned* keys, unsigned* idx, cudaStream_t st);
+// re-sort gather that also deposits the gathered state into mesh (FP64) or
+// qmesh (mixed int64); the target must be zeroed
+void launch_gather_deposit(int nf, bool mixed, const DevParams& P, const DevState& src, const DevState& dst,
+                           const unsigned* perm, double* mesh, long long* qmesh, cudaStream_t st);
 void launch_gather_state(int nf, bool mixed, const DevState& src, const DevState& dst, const unsigned* perm,
                          cudaStream_t st);
 

@@ -24,6 +24,7 @@
 
 #include <climits>
 #include <cstdio>
+#include <type_traits>
 
 namespace emu {
 
@@ -525,8 +526,9 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
             make_stencil<double>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
-                                        [](double a, int) -> double { return a; }, s == 4);
+    if (mesh_out)   // (null: the stage-4 deposit is made by the re-sort gather)
+        tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
+                                            [](double a, int) -> double { return a; }, s == 4);
 }
 
 // FP64 potential of one species (potential_fp64 restricted to species sp)
@@ -640,8 +642,9 @@ __device__ __forceinline__ void rk4_stage_body_split(const DevParams& P, const D
             make_stencil<double>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    tile_deposit_block_split<NF, SWt, double>(P, mesh_out, active, st, sp, fN, vx, vy, vz,
-                                              [](double a, int) -> double { return a; }, s == 4);
+    if (mesh_out)
+        tile_deposit_block_split<NF, SWt, double>(P, mesh_out, active, st, sp, fN, vx, vy, vz,
+                                                  [](double a, int) -> double { return a; }, s == 4);
 }
 
 // Two flavors, 1D stencils: species-split kernels (2 kBlock threads per
@@ -959,7 +962,8 @@ __device__ __forceinline__ void potential_si32(const DevParams& P, const float* 
 }
 
 template <int NF, int WX, int WY, int WZ>
-__global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevState S, int s,
+// (1D: 5 CTAs per SM at 96 registers beat 4 at 128 despite the spills)
+__global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S, int s,
                                                             const float* __restrict__ gmesh,
                                                             long long* __restrict__ qout,
                                                             const long long* __restrict__ qdt, StepCtl* ctl,
@@ -1110,7 +1114,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage_mixed(DevParams P, DevS
             make_stencil<float>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4);
+    if (qout) tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4);
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
 }
 
@@ -1220,6 +1224,71 @@ __global__ void k_gather_state(DevState src, DevState dst, const unsigned* __res
         for (int d = 0; d < 3; d++) dst.vhat32[d][i] = src.vhat32[d][j];
         for (int sp = 0; sp < 2; sp++) dst.N32[sp][i] = src.N32[sp][j];
     }
+}
+
+// Re-sort gather fused with the deposit of the gathered (new, cell-sorted)
+// state: the deposit the last RK stage makes otherwise at the moved
+// positions, where the particles are out of stencil order.  Same values as
+// that deposit (f N and v in the path's precision).
+template <int NF, int WX, int WY, int WZ, bool MIXED>
+__global__ void __launch_bounds__(kBlock) k_gather_deposit(DevParams P, DevState src, DevState dst,
+                                                           const unsigned* __restrict__ perm,
+                                                           double* __restrict__ mesh, long long* __restrict__ qmesh)
+{
+    using SWt = SW<WX, WY, WZ>;
+    using R = typename std::conditional<MIXED, float, double>::type;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < src.n;
+    Stencil<R> st{};
+    R fN[NS] = {};
+    R vx = 0, vy = 0, vz = 0;
+    if (active) {
+        const long long j = perm[i];
+        double x[3];
+        for (int d = 0; d < 3; d++) {
+            x[d] = src.pos[d][j];
+            dst.pos[d][i] = x[d];
+            dst.vhat[d][i] = src.vhat[d][j];
+        }
+        dst.time[i] = src.time[j];
+        for (int d = 0; d < 4; d++) dst.pup[d][i] = src.pup[d][j];
+        double Nn[2];
+        for (int sp = 0; sp < 2; sp++) {
+            Nn[sp] = src.Nn[sp][j];
+            dst.Nn[sp][i] = Nn[sp];
+            dst.Ll[sp][i] = src.Ll[sp][j];
+        }
+        dst.vscale[i] = src.vscale[j];
+        dst.id[i] = src.id[j];
+        float N32[2] = {0.f, 0.f};
+        if constexpr (MIXED) {
+            for (int d = 0; d < 3; d++) dst.vhat32[d][i] = src.vhat32[d][j];
+            for (int sp = 0; sp < 2; sp++) {
+                N32[sp] = src.N32[sp][j];
+                dst.N32[sp][i] = N32[sp];
+            }
+            vx = src.vhat32[0][j];
+            vy = src.vhat32[1][j];
+            vz = src.vhat32[2][j];
+        } else {
+            vx = src.vhat[0][j];
+            vy = src.vhat[1][j];
+            vz = src.vhat[2][j];
+        }
+#pragma unroll
+        for (int c = 0; c < NS; c++) {
+            const double f = src.f0[c * src.cap + j];
+            dst.f0[c * dst.cap + i] = f;
+            if constexpr (MIXED) fN[c] = (float)f * N32[c / NH];
+            else fN[c] = f * Nn[c / NH];
+        }
+        make_stencil<R>(P, x[0], x[1], x[2], st);
+    }
+    if constexpr (MIXED) tile_deposit_block<NF, SWt, float>(P, qmesh, active, st, fN, vx, vy, vz, QuantConv{P});
+    else
+        tile_deposit_block<NF, SWt, double>(P, mesh, active, st, fN, vx, vy, vz,
+                                            [](double a, int) -> double { return a; });
 }
 
 __global__ void k_mixed_shadow(DevState S)
@@ -1379,6 +1448,25 @@ cudaError_t launch_rk4_step_coop_t(const DevParams& P, const DevState& S, double
                                           args, bytes, st);
     });
     return err;
+}
+
+template <int NF>
+void launch_gather_deposit_t(bool mixed, const DevParams& P, const DevState& src, const DevState& dst,
+                             const unsigned* perm, double* mesh, long long* qmesh, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, {
+        if (mixed) {
+            constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>();
+            smem_optin(k_gather_deposit<NF, WXv, WYv, WZv, true>, bytes);
+            k_gather_deposit<NF, WXv, WYv, WZv, true><<<grid_for(src.n), kBlock, bytes, st>>>(P, src, dst, perm,
+                                                                                             mesh, qmesh);
+        } else {
+            constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
+            smem_optin(k_gather_deposit<NF, WXv, WYv, WZv, false>, bytes);
+            k_gather_deposit<NF, WXv, WYv, WZv, false><<<grid_for(src.n), kBlock, bytes, st>>>(P, src, dst, perm,
+                                                                                              mesh, qmesh);
+        }
+    });
 }
 
 template <int NF>

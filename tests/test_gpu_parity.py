@@ -77,7 +77,7 @@ def _c2_small(ncz=16, ndirs=20, **kw):
     return p
 
 
-@pytest.mark.parametrize("resort,fused", [(0, 2), (1, 2), (3, 2), (0, 1), (3, 1)])
+@pytest.mark.parametrize("resort,fused", [(0, 2), (1, 2), (3, 2), (0, 1), (1, 1), (3, 1)])
 def test_evolve_matches_oracle(resort, fused):
     """device-resident loop (cooperative step kernel or CUDA graph of stage
     kernels, device dt) vs the oracle's evolve"""
@@ -93,6 +93,24 @@ def test_evolve_matches_oracle(resort, fused):
         out = c.get_particles()
     assert colwise_rel(out, ref) < 1e-11
     assert colwise_rel(out[:, flavor_cols(2)], ref[:, flavor_cols(2)]) < 1e-11
+
+
+def test_evolve_3d_matches_oracle():
+    """3 flavors, 3D TSC: re-sort every step (automatic), the new state
+    deposited by the re-sort gather"""
+    p = W.c5_3d(n=4, ndirs=5, mixed=False)
+    parts = api.init_particles(p)
+    o = Oracle(p)
+    ref, t_ref, _, _ = o.evolve(parts, 6)
+    with api.Context(p) as c:
+        c.load_particles(parts)
+        info = c.evolve(6)
+        assert info.status == 0 and info.steps_done == 6
+        assert abs(info.time - t_ref) <= 1e-12 * t_ref
+        out = c.get_particles()
+        mesh = c.get_mesh()
+    assert colwise_rel(out, ref) < 1e-11
+    assert colwise_rel(out[:, flavor_cols(3)], ref[:, flavor_cols(3)]) < 1e-11
 
 
 def test_evolve_end_time_clipping():
