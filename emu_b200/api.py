@@ -130,6 +130,7 @@ SIGNATURES = {
     "emu_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "emu_deposit_noalloc": (ctypes.c_int, [_P(EmuParams), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "emu_init_particles_device": (ctypes.c_int, [ctypes.c_void_p]),
     "emu_comm_id": (ctypes.c_int, [ctypes.c_char_p]),
     "emu_attach_comm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
     "emu_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D,
@@ -357,6 +358,10 @@ class Context:
         if code & ~(EMU_ERR_TRACE | EMU_ERR_NEGDIAG | EMU_ERR_LENGTH | EMU_ERR_DT):
             self._ck(code, "emu_evolve")
         return info
+
+    def init_particles_device(self):
+        """InitParticles on the device, loaded into this context"""
+        self._ck(self.lib.emu_init_particles_device(self.h), "emu_init_particles_device")
 
     def attach_comm(self, comm_id, rank, nranks):
         """join a particle-sharding communicator (before load_particles)"""

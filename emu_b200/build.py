@@ -25,8 +25,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
 
 SOURCES = ["emu_k_fp64_3.cu", "emu_k_mixed_3.cu", "emu_adjoint.cu", "emu_k_fp64_2.cu", "emu_k_mixed_2.cu",
-           "emu_k_misc.cu", "emu_capi.cu", "emu_comm.cu", "emu_noalloc.cu", "emu_host.cpp", "emu_init.cpp"]
-HEADERS = ["emu_device.cuh", "emu_kernels.cuh", "emu_kernels_impl.cuh", "emu_context.cuh", "emu_host.h"]
+           "emu_k_misc.cu", "emu_capi.cu", "emu_comm.cu", "emu_noalloc.cu", "emu_init_device.cu", "emu_host.cpp",
+           "emu_init.cpp"]
+# the device initial-condition generator must round like the host one
+EXTRA = {"emu_init_device.cu": ["-fmad=false"]}
+HEADERS = ["emu_device.cuh", "emu_kernels.cuh", "emu_kernels_impl.cuh", "emu_context.cuh", "emu_host.h",
+           "emu_init_record.h"]
 
 
 def _stale(out, deps):
@@ -42,7 +46,7 @@ def _compile(src, verbose_ptxas):
     deps = [path] + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "emu_b200.h")]
     if not _stale(obj, deps):
         return obj, ""
-    cmd = [NVCC] + ARCH + COMMON + ["-c", path, "-o", obj]
+    cmd = [NVCC] + ARCH + COMMON + EXTRA.get(src, []) + ["-c", path, "-o", obj]
     if src.endswith(".cu"):
         cmd += ["--extended-lambda", "-Xptxas", "-warn-spills"]
         if verbose_ptxas:

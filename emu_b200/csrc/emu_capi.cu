@@ -453,6 +453,55 @@ int emu_ctx::resort_now(emu_context* ctx, unsigned* perm)
     return EMU_OK;
 }
 
+int emu_ctx::reserve(emu_context* ctx, int64_t n)
+{
+    if (n > (int64_t)INT_MAX) return fail(ctx, EMU_ERR_LIMIT, "load: more than 2^31-1 particles");
+    if (n <= 0) return fail(ctx, EMU_ERR_ARG, "load: no particles");
+    int r;
+    if ((r = ensure_capacity(ctx, n))) return r;
+    return ensure_aos(ctx, n);
+}
+
+// the particles are in ctx->aos (records, load order); pupt_min and the
+// weight sums/maxima are this rank's
+int emu_ctx::load_from_aos(emu_context* ctx, int64_t n, double pupt_min, const double tot_in[2],
+                           const double mx_in[2])
+{
+    int r;
+    // (over all ranks of a sharded run)
+    double vmin_neg = -pupt_min;
+    if ((r = emu_ctx_reduce_scalars(ctx, &vmin_neg, 1, 1))) return r;
+    ctx->P.vvac_max = emu_host::vvac_from_pupt_min(ctx->prm, -vmin_neg);
+    if (ctx->mixed) {
+        std::string why;
+        double tot[2] = {tot_in[0], tot_in[1]}, mx[2] = {mx_in[0], mx_in[1]};
+        if ((r = emu_ctx_reduce_scalars(ctx, tot, 2, 0))) return r;
+        if ((r = emu_ctx_reduce_scalars(ctx, mx, 2, 1))) return r;
+        if (!emu_host::fixed_point_scales_from(tot, mx, ctx->P.q_scale, ctx->P.q_unscale, why))
+            return fail(ctx, EMU_ERR_LIMIT, "load: " + why);
+    }
+    emu::launch_cell_keys(ctx->P, ctx->aos, ctx->nreal, n, ctx->keys, ctx->idx, ctx->stream);
+    if ((r = sort_perm(ctx, n))) return r;
+    ctx->cur = 0;
+    DevState& S = ctx->S[0];
+    S.n = n;
+    ctx->S[1].n = n;
+    emu::launch_pack(ctx->nf, ctx->P, ctx->aos, ctx->idx2, n, S, ctx->stream);
+    if (ctx->mixed) emu::launch_mixed_shadow(ctx->nf, S, ctx->stream);
+    if ((r = check_launch(ctx, "pack"))) return r;
+    // (step graphs re-capture themselves when P or S differ from their capture)
+    // fused == 2: one cooperative launch per step when the grid fits
+    // (a sharded run reduces every deposit between stages: per-stage kernels)
+    ctx->coop = !ctx->mixed && !ctx->comm && ctx->prm.fused == 2 && rk4_fused(ctx) &&
+                emu::coop_step_fits(ctx->nf, ctx->P, n);
+    ctx->loaded = true;
+    ctx->adj_valid = false;
+    ctx->steps_since_sort = 0;
+    if ((r = deposit_current(ctx))) return r;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return EMU_OK;
+}
+
 extern "C" {
 
 int emu_abi_version(void) { return EMU_B200_ABI_VERSION; }
@@ -583,49 +632,17 @@ int emu_synchronize(emu_context* ctx)
 int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
 {
     if (!ctx || (n > 0 && !records) || n < 0) return fail(ctx, EMU_ERR_ARG, "emu_load_particles: bad arguments");
-    if (n > (int64_t)INT_MAX) return fail(ctx, EMU_ERR_LIMIT, "emu_load_particles: more than 2^31-1 particles");
-    if (n == 0) return fail(ctx, EMU_ERR_ARG, "emu_load_particles: no particles");
     int r;
-    if ((r = ensure_capacity(ctx, n))) return r;
-    if ((r = ensure_aos(ctx, n))) return r;
+    if ((r = emu_ctx::reserve(ctx, n))) return r;
     CU(cudaMemcpyAsync(ctx->aos, records, sizeof(double) * (size_t)n * ctx->nreal, cudaMemcpyHostToDevice,
                        ctx->stream));
     // host-side scalars derived from the particles: Vvac_max (Init.cpp:657-660)
-    // and, for the mixed path, the fixed-point scales
-    // (over all ranks of a sharded run)
-    double vvac = 0.0;
-    emu_vvac_max(&ctx->prm, records, n, &vvac);
-    if ((r = emu_ctx_reduce_scalars(ctx, &vvac, 1, 1))) return r;
-    ctx->P.vvac_max = vvac;
-    if (ctx->mixed) {
-        std::string why;
-        double tot[2], mx[2];
-        emu_host::weight_totals(ctx->prm, records, n, tot, mx);
-        if ((r = emu_ctx_reduce_scalars(ctx, tot, 2, 0))) return r;
-        if ((r = emu_ctx_reduce_scalars(ctx, mx, 2, 1))) return r;
-        if (!emu_host::fixed_point_scales_from(tot, mx, ctx->P.q_scale, ctx->P.q_unscale, why))
-            return fail(ctx, EMU_ERR_LIMIT, "emu_load_particles: " + why);
-    }
-    emu::launch_cell_keys(ctx->P, ctx->aos, ctx->nreal, n, ctx->keys, ctx->idx, ctx->stream);
-    if ((r = sort_perm(ctx, n))) return r;
-    ctx->cur = 0;
-    DevState& S = ctx->S[0];
-    S.n = n;
-    ctx->S[1].n = n;
-    emu::launch_pack(ctx->nf, ctx->P, ctx->aos, ctx->idx2, n, S, ctx->stream);
-    if (ctx->mixed) emu::launch_mixed_shadow(ctx->nf, S, ctx->stream);
-    if ((r = check_launch(ctx, "pack"))) return r;
-    // (step graphs re-capture themselves when P or S differ from their capture)
-    // fused == 2: one cooperative launch per step when the grid fits
-    // (a sharded run reduces every deposit between stages: per-stage kernels)
-    ctx->coop = !ctx->mixed && !ctx->comm && ctx->prm.fused == 2 && rk4_fused(ctx) &&
-                emu::coop_step_fits(ctx->nf, ctx->P, n);
-    ctx->loaded = true;
-    ctx->adj_valid = false;
-    ctx->steps_since_sort = 0;
-    if ((r = deposit_current(ctx))) return r;
-    CU(cudaStreamSynchronize(ctx->stream));
-    return EMU_OK;
+    // and, for the mixed path, the weight sums behind the fixed-point scales
+    double pupt_min = INFINITY;
+    for (int64_t q = 0; q < n; q++) pupt_min = std::min(pupt_min, records[q * ctx->nreal + 3 + 7]);
+    double tot[2] = {0, 0}, mx[2] = {0, 0};
+    if (ctx->mixed) emu_host::weight_totals(ctx->prm, records, n, tot, mx);
+    return emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx);
 }
 
 int emu_get_particles(emu_context* ctx, double* records, int64_t n)

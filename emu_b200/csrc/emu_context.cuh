@@ -79,6 +79,12 @@ int emu_ctx_reduce_scalars(emu_context* ctx, double* v, int n, int op);
 // destroys the attached communicator (emu_destroy, after the graphs)
 void emu_ctx_comm_free(emu_context* ctx);
 namespace emu_ctx {
+// device capacity for n particles (particle arrays and the record staging)
+int reserve(emu_context* ctx, int64_t n);
+// finish a load whose n records are in ctx->aos: global scalars (Vvac_max
+// from this rank's smallest pupt, mixed fixed-point scales from its weight
+// sums and maxima), cell sort, pack, initial deposit
+int load_from_aos(emu_context* ctx, int64_t n, double pupt_min, const double tot[2], const double mx[2]);
 // re-sort the particles by cell now; when perm is not null it receives the
 // gather permutation (new slot i holds old slot perm[i])
 int resort_now(emu_context* ctx, unsigned* perm);

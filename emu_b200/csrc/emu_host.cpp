@@ -444,6 +444,16 @@ const double kDeg = M_PI / 180.;
 
 }  // namespace
 
+double emu_host::vvac_from_pupt_min(const emu_params& p, double pupt_min)
+{
+    const int nf = p.nflavors;
+    double h[9] = {0};
+    h[herm_re(nf, 0, 0)] = p.mass1 * p.mass1;
+    h[herm_re(nf, 1, 1)] = p.mass2 * p.mass2;
+    if (nf == 3) h[herm_re(nf, 2, 2)] = p.mass3 * p.mass3;
+    return su_length(nf, h) * emu_host::c4() / pupt_min;
+}
+
 extern "C" {
 
 void emu_params_default(emu_params* p)
@@ -589,17 +599,14 @@ int emu_parse_inputs(const char* path, int n_overrides, const char* const* overr
     return EMU_OK;
 }
 
+
 int emu_vvac_max(const emu_params* p, const double* records, int64_t n, double* out)
 {
     if (!p || !out || (n > 0 && !records)) return EMU_ERR_ARG;
     const int nf = p->nflavors, nr = 3 + 8 + 2 * (2 + nf * nf);
     double pupt_min = INFINITY;
     for (int64_t i = 0; i < n; i++) pupt_min = std::min(pupt_min, records[i * nr + 3 + 7]);
-    double h[9] = {0};
-    h[herm_re(nf, 0, 0)] = p->mass1 * p->mass1;
-    h[herm_re(nf, 1, 1)] = p->mass2 * p->mass2;
-    if (nf == 3) h[herm_re(nf, 2, 2)] = p->mass3 * p->mass3;
-    *out = su_length(nf, h) * emu_host::c4() / pupt_min;
+    *out = emu_host::vvac_from_pupt_min(*p, pupt_min);
     return EMU_OK;
 }
 

@@ -4,8 +4,10 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "emu_b200.h"
+#include "emu_init_record.h"
 
 namespace emu_host {
 
@@ -33,6 +35,15 @@ bool fixed_point_scales(const emu_params& p, const double* records, long long n,
 void weight_totals(const emu_params& p, const double* records, long long n, double total[2], double mx[2]);
 bool fixed_point_scales_from(const double totals[2], const double maxima[2], double scale[2], double unscale[2],
                              std::string& why);
+
+// Vvac_max (FlavoredNeutrinoContainerInit.cpp:657-660) from the smallest
+// particle energy
+double vvac_from_pupt_min(const emu_params& p, double pupt_min);
+
+// inputs of the initial-particle generator (emu_init_record.h); total =
+// particle count
+bool make_init_spec(const emu_params& p, emu_init::InitSpec& s, std::vector<double>& dirs, long long& total,
+                    std::string& why);
 
 bool write_plotfile(const emu_params& p, const char* dir, double time, int step, const double* mesh,
                     const double* records, long long n, std::string& why);

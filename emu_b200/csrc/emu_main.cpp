@@ -67,14 +67,14 @@ int main(int argc, char** argv)
         recs.resize((size_t)n * emu_nreal(p.nflavors));
         if ((r = emu_read_particles(p.restart_dir, p.nflavors, recs.data(), n, &n, &t0, &step0)))
             return die(nullptr, r, "restart");
-    } else {
-        if ((r = emu_init_particles(&p, nullptr, 0, &n))) return die(nullptr, r, "InitParticles");
-        recs.resize((size_t)n * emu_nreal(p.nflavors));
-        if ((r = emu_init_particles(&p, recs.data(), n, &n))) return die(nullptr, r, "InitParticles");
     }
     emu_context* ctx = nullptr;
     if ((r = emu_create(&p, &ctx))) return die(nullptr, r, "emu_create");
-    if ((r = emu_load_particles(ctx, recs.data(), n))) return die(ctx, r, "emu_load_particles");
+    if (p.do_restart) {
+        if ((r = emu_load_particles(ctx, recs.data(), n))) return die(ctx, r, "emu_load_particles");
+    } else if ((r = emu_init_particles_device(ctx))) {   // InitParticles, on the device
+        return die(ctx, r, "InitParticles");
+    }
     if (!p.do_restart && (r = emu_write_plotfile(ctx, plot_name(step0).c_str(), t0, step0, 1)))
         return die(ctx, r, "WritePlotFile");
     std::printf("Done. \nStarting timestepping loop... \n");

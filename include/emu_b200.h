@@ -138,6 +138,13 @@ int emu_parse_inputs(const char* path, int n_overrides, const char* const* overr
 /* Initial particles on the host (replaces FlavoredNeutrinoContainer::InitParticles,
  * FlavoredNeutrinoContainerInit.cpp:136-661).  With out == NULL only *n_out is set. */
 int emu_init_particles(const emu_params* p, double* out, int64_t capacity, int64_t* n_out);
+/* InitParticles on the device: the particles emu_init_particles would
+ * return, generated in device memory and loaded into ctx (replaces
+ * emu_init_particles + emu_load_particles without the host round trip).
+ * Bit-identical records except where simulation types 3 and 5 evaluate
+ * sin / exp.  A context attached to a communicator generates the particles
+ * of global indices rank, rank + nranks, ... (its shard). */
+int emu_init_particles_device(emu_context* ctx);
 /* Vvac_max of a particle set (FlavoredNeutrinoContainerInit.cpp:657-660). */
 int emu_vvac_max(const emu_params* p, const double* records, int64_t n, double* out);
 
