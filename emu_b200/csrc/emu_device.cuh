@@ -1,7 +1,7 @@
 // emu_device.cuh -- device-side building blocks of the Emu evolution path on
 // sm_100a: Hermitian component layout, shape factors, the interpolated
 // potential, the commutator right-hand side, renormalisation and the
-// warp-cooperative deposit.
+// shared-memory tile deposit.
 //
 // Reference semantics (paths relative to the Emu tree):
 //   shape factors        Source/ParticleInterpolator.H:34-131
@@ -263,36 +263,6 @@ struct SW {
     }
 };
 
-// Warp reduction of 32 values per lane, produced on the fly by gen(i):
-// afterwards lane l holds the sum over the warp of value index l (recursive
-// halving, 31 shuffles per 32 values, at most 16 values live).
-template <class T, class Gen>
-__device__ __forceinline__ T warp_transpose_sum(Gen gen)
-{
-    const int lane = threadIdx.x & 31;
-    T v[16];
-    {
-        const bool upper = (lane & 16) != 0;
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const T a = gen(i), b = gen(i + 16);
-            const T send = upper ? a : b;
-            const T keep = upper ? b : a;
-            v[i] = keep + __shfl_xor_sync(kFull, send, 16);
-        }
-    }
-#pragma unroll
-    for (int off = 8; off >= 1; off >>= 1) {
-        const bool upper = (lane & off) != 0;
-#pragma unroll
-        for (int i = 0; i < off; i++) {
-            const T send = upper ? v[i] : v[i + off];
-            const T keep = upper ? v[i + off] : v[i];
-            v[i] = keep + __shfl_xor_sync(kFull, send, off);
-        }
-    }
-    return v[0];
-}
 
 __device__ __forceinline__ void atomic_add_mesh(double* p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add_mesh(long long* p, long long v)
@@ -399,14 +369,13 @@ struct RunAcc<float, S, SP> {
 };
 
 // Phase B of the tile deposit: thread q owns mesh component q of every
-// stencil cell; it walks its stream of records (contiguous, in key order
-// through sidx when given), sums each run
+// stencil cell; it walks its stream of records (contiguous), sums each run
 // of equal stencil keys in registers and adds the run total with one atomic
 // per (cell, component).  Inside a run, aligned groups of four records with
 // the run's key are summed without per-record key tests.
 template <int NF, int BLOCK, int NTILE, class SWt, class R, class T, class Conv>
-__device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const int* sidx,
-                                             const R* srec, int ntile, Conv conv)
+__device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const R* srec, int ntile,
+                                             Conv conv)
 {
     using TR = TileRec<NF, SWt, R>;
     constexpr int NH = NF * NF, NS = 2 * NH, ND = 8 * NH, RW = TR::RW, SP = TR::SP;
@@ -438,7 +407,7 @@ __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const 
                 }
     };
     auto add_one = [&](int i) {
-        const R* r = srec + (sidx ? sidx[i] : i) * RW;
+        const R* r = srec + i * RW;
         const R b = r[boff];
         const R qv = dir == 0 ? b : b * r[voff];
         R w[SP];
@@ -500,64 +469,5 @@ __device__ __forceinline__ void tile_record(R* srec, int* skey, int i, int key, 
     r[SP + NS + 2] = vz;
 }
 
-template <int ND, int MAXG, class SWt, class T, class W, class ValFn, class Conv>
-__device__ __forceinline__ void warp_deposit(const DevParams& P, T* mesh, int key, const Stencil<W>& st,
-                                             ValFn val, Conv conv)
-{
-    const int lane = threadIdx.x & 31;
-    constexpr int NR = (ND + 31) / 32;
-    const unsigned peers = __match_any_sync(kFull, key);
-    const bool leader = (__ffs(peers) - 1) == lane;
-    unsigned leaders = __ballot_sync(kFull, leader && key >= 0);
-    const int ng = __popc(leaders);
-    if (ng == 0) return;
-    if (ng <= MAXG) {
-        while (leaders) {
-            const int ld = __ffs(leaders) - 1;
-            leaders &= leaders - 1;
-            const int gkey = __shfl_sync(kFull, key, ld);
-            const bool mine = (key == gkey);
-            const int bx = gkey % P.n[0];
-            const int by = (gkey / P.n[0]) % P.n[1];
-            const int bz = gkey / (P.n[0] * P.n[1]);
-#pragma unroll
-            for (int kk = 0; kk < SWt::MZ; kk++)
-#pragma unroll
-                for (int jj = 0; jj < SWt::MY; jj++)
-#pragma unroll
-                    for (int ii = 0; ii < SWt::MX; ii++) {
-                        if (!SWt::on(P, ii, jj, kk)) continue;
-                        const W wgt = mine ? st.wx[ii] * st.wy[jj] * st.wz[kk] : (W)0;
-                        const long long cell = cell_of(P, bx, by, bz, ii, jj, kk);
-#pragma unroll
-                        for (int r = 0; r < NR; r++) {
-                            const T tot = warp_transpose_sum<T>([&](int i) -> T {
-                                const int q = r * 32 + i;
-                                return (mine && q < ND) ? conv(wgt, val(q), q) : (T)0;
-                            });
-                            const int q = r * 32 + lane;
-                            if (q < ND && tot != (T)0) atomic_add_mesh(&mesh[cell * ND + q], tot);
-                        }
-                    }
-        }
-    } else {
-        if (key < 0) return;
-#pragma unroll
-        for (int kk = 0; kk < SWt::MZ; kk++)
-#pragma unroll
-            for (int jj = 0; jj < SWt::MY; jj++)
-#pragma unroll
-                for (int ii = 0; ii < SWt::MX; ii++) {
-                    if (!SWt::on(P, ii, jj, kk)) continue;
-                    const W wgt = st.wx[ii] * st.wy[jj] * st.wz[kk];
-                    const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
-#pragma unroll
-                    for (int q = 0; q < ND; q++) {
-                        const T c = conv(wgt, val(q), q);
-                        if (c != (T)0) atomic_add_mesh(&mesh[cell * ND + q], c);
-                    }
-                }
-    }
-}
 
 }  // namespace emu

@@ -1,13 +1,19 @@
-// emu_kernels.cu -- CUDA kernels (sm_100a) for Emu's per-step evolution path.
+// emu_kernels_impl.cuh -- CUDA kernels (sm_100a) for Emu's per-step evolution
+// path (instantiated per flavor count in emu_k_fp64_<nf>.cu,
+// emu_k_mixed_<nf>.cu and emu_k_misc.cu).
 //
-// One thread per particle; particles are cell-sorted so that the lanes of a
-// warp share stencils and their deposits are reduced in registers.
+// One thread per particle (two for the species-split kernels); particles are
+// cell-sorted so that a CTA's particles share stencils and their deposits are
+// summed per run in registers (the tile deposit, emu_device.cuh).
 //   k_rk4_stage<NF,W>        fused RK4 stage (FP64): interpolate the stage
 //                            mesh, -i[H,rho], RK bookkeeping, deposit of the
 //                            next stage state.  Stage 4 also combines, wraps,
 //                            renormalises, deposits the new state for the
 //                            next step and (device-resident loop) reduces
 //                            compute_dt over the stage-4 mesh.
+//   k_rk4_stage_split<2,W>   the same, 2 threads per particle (nu, nubar)
+//   k_rk4_step_coop*         a whole step in one cooperative launch
+//   k_gather_deposit         re-sort gather + deposit of the new state
 //   k_rk4_stage_mixed<NF,W>  the same with FP32 interpolation and
 //                            self-interaction commutator, FP64 vacuum+matter
 //                            commutator and state, int64 fixed-point deposit
@@ -350,7 +356,7 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
     }
     tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
     __syncthreads();
-    tile_deposit<NF, kBlock, kBlock, SWt, R, T>(P, mesh, skey, nullptr, srec, kBlock, conv);
+    tile_deposit<NF, kBlock, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
 }
 
 // The same for a species-split CTA (kBlock particles, 2 kBlock threads:
@@ -402,7 +408,7 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
 #pragma unroll
     for (int e = 0; e < NH; e++) r[SP + sp * NH + e] = fNs[e];
     __syncthreads();
-    tile_deposit<NF, NT, kBlock, SWt, R, T>(P, mesh, skey, nullptr, srec, kBlock, conv);
+    tile_deposit<NF, NT, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
 }
 
 // ===========================================================================
