@@ -324,7 +324,8 @@ def run_emu(args):
     e2e = None
     if not args.no_e2e:
         import threading
-        pipes = args.e2e_pipes if ws == 1 else 1
+        # (pinned host buffers of all batches within 32 GB)
+        pipes = max(1, min(args.e2e_pipes, int(32e9 // (2 * recs.nbytes)))) if ws == 1 else 1
         ne = min(args.steps, args.e2e_steps)
         lanes = []
         for k in range(pipes):
@@ -475,7 +476,7 @@ def main():
                     help="particle-sharded path even on one GPU (a one-rank communicator)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--e2e-pipes", type=int, default=4,
+    ap.add_argument("--e2e-pipes", type=int, default=8,
                     help="batches in flight for the end-to-end figure (one GPU)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
