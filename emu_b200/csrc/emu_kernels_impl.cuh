@@ -32,6 +32,8 @@
 #include <cstdio>
 #include <type_traits>
 
+#include <utility>
+
 namespace emu {
 
 namespace {
@@ -139,6 +141,20 @@ __device__ __forceinline__ void zero_slice(T* buf, long long n)
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) buf[i] = (T)0;
 }
+
+// Programmatic dependent launch (sm_90+).  The stage kernels are launched
+// with programmatic stream serialization: a stage may start while the
+// previous kernel of the stream drains.  Before grid_dep_wait it only loads
+// fields that no kernel of the same step writes (positions, velocities,
+// weights, the state at the start of the step: written by the previous
+// step's last stage or a re-sort, which completed before the previous
+// kernel passed its own wait), through L2 (ld.global.cg, no stale L1 lines);
+// after it, everything the previous kernel wrote is complete and visible.
+// grid_dep_launch lets the next kernel start its own prologue; it comes after
+// the wait, so that a prologue never overlaps a kernel two launches back.
+// Without the launch attribute both are no-ops.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // ===========================================================================
 // compute_dt pieces (Evolve.cpp:57-124 + compute_dt fill)
@@ -417,50 +433,70 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
 template <int NF, class SWt>
 __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevState& S, int s,
                                                const double* __restrict__ mesh_in, double* __restrict__ mesh_out,
-                                               double* mesh_zero, long long nzero, StepCtl* ctl, double dt)
+                                               double* mesh_zero, long long nzero, StepCtl* ctl, double dt,
+                                               int dt_mode = -1)
 {
     constexpr int NH = NF * NF, NS = 2 * NH;
     // whole-state preload where it fits the register budget (two flavors,
     // one-dimensional stencil)
     constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
-    zero_slice(mesh_zero, nzero);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
     const long long cap = S.cap;
 
+    // prologue: fields that no kernel of this step writes
     Stencil<double> st{};
     double fN[NS] = {};
-    double vx = 0, vy = 0, vz = 0;
+    double vx = 0, vy = 0, vz = 0, x = 0, y = 0, z = 0, vsc = 0;
+    double Nsp[2] = {0, 0}, Lsp[2] = {0, 0}, t_in = 0;
+    constexpr int PRE = PRELOAD ? NS : 1;
+    double fc[PRE], yv[PRE], av[PRE];
+    const bool hoist = PRELOAD && s == 4;
     if (active) {
-        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
-        vx = S.vhat[0][p];
-        vy = S.vhat[1][p];
-        vz = S.vhat[2][p];
-        // the stage's per-particle loads are issued together (one memory
-        // round trip); the state arrays never alias
+        x = __ldcg(S.pos[0] + p);
+        y = __ldcg(S.pos[1] + p);
+        z = __ldcg(S.pos[2] + p);
+        vx = __ldcg(S.vhat[0] + p);
+        vy = __ldcg(S.vhat[1] + p);
+        vz = __ldcg(S.vhat[2] + p);
+        vsc = __ldcg(S.vscale + p);
+        Nsp[0] = __ldcg(S.Nn[0] + p);
+        Nsp[1] = __ldcg(S.Nn[1] + p);
+        if (hoist) {
+            Lsp[0] = __ldcg(S.Ll[0] + p);
+            Lsp[1] = __ldcg(S.Ll[1] + p);
+            t_in = __ldcg(S.time + p);
+        }
+        if constexpr (PRELOAD) {
+            if (s > 1) {
+#pragma unroll
+                for (int c = 0; c < NS; c++) yv[c] = __ldcg(S.f0 + c * cap + p);
+            }
+        }
+        make_stencil<double>(P, x, y, z, st);
+    }
+    grid_dep_wait();
+    grid_dep_launch();
+    // stage 4 of the device-resident loop: compute_dt on the stage-4 mesh
+    // (main.cpp:193-198), which this kernel only reads; every block has read
+    // this step's dt before it takes part
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+    zero_slice(mesh_zero, nzero);
+    if (active) {
+        // the stage's remaining per-particle loads are issued together (one
+        // memory round trip); the state arrays never alias
         const double* __restrict__ fin = s == 1 ? S.f0 : S.fs;
         const double* __restrict__ f0p = S.f0;
         const double* __restrict__ accp = S.acc;
-        const double vsc = S.vscale[p];
-        const double Nsp[2] = {S.Nn[0][p], S.Nn[1][p]};
-        const bool hoist = PRELOAD && s == 4;
-        const double Lsp[2] = {hoist ? S.Ll[0][p] : 0.0, hoist ? S.Ll[1][p] : 0.0};
-        const double t_in = hoist ? S.time[p] : 0.0;
-        constexpr int PRE = PRELOAD ? NS : 1;
-        double fc[PRE], yv[PRE], av[PRE];
         if constexpr (PRELOAD) {
 #pragma unroll
             for (int c = 0; c < NS; c++) fc[c] = fin[c * cap + p];
             if (s > 1) {
 #pragma unroll
-                for (int c = 0; c < NS; c++) {
-                    yv[c] = f0p[c * cap + p];
-                    av[c] = accp[c * cap + p];
-                }
+                for (int c = 0; c < NS; c++) av[c] = accp[c * cap + p];
             }
         }
         double V[NS];
-        make_stencil<double>(P, x, y, z, st);
         potential_fp64<NF, SWt>(P, mesh_in, st, vx, vy, vz, vsc, V);
         const double bw = dt * kRK4B[s - 1];
         const double aw = s < 4 ? dt * kRK4A[s] : 0.0;
@@ -570,36 +606,47 @@ __device__ __forceinline__ void potential_fp64_sp(const DevParams& P, const doub
 template <int NF, class SWt>
 __device__ __forceinline__ void rk4_stage_body_split(const DevParams& P, const DevState& S, int s,
                                                      const double* __restrict__ mesh_in, double* __restrict__ mesh_out,
-                                                     double* mesh_zero, long long nzero, StepCtl* ctl, double dt)
+                                                     double* mesh_zero, long long nzero, StepCtl* ctl, double dt,
+                                                     int dt_mode = -1)
 {
     constexpr int NH = NF * NF;
-    zero_slice(mesh_zero, nzero);
     const int sp = threadIdx.x / kBlock;
     const long long p = (long long)blockIdx.x * kBlock + threadIdx.x % kBlock;
     const bool active = p < S.n;
     const long long cap = S.cap;
+    // prologue: fields that no kernel of this step writes
     Stencil<double> st{};
     double fN[NH] = {};
-    double vx = 0, vy = 0, vz = 0;
+    double vx = 0, vy = 0, vz = 0, x = 0, y = 0, z = 0, vsc = 0, Ns = 0, Ls = 0, t_in = 0;
+    double y0[NH];
     if (active) {
-        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
-        vx = S.vhat[0][p];
-        vy = S.vhat[1][p];
-        vz = S.vhat[2][p];
+        x = __ldcg(S.pos[0] + p);
+        y = __ldcg(S.pos[1] + p);
+        z = __ldcg(S.pos[2] + p);
+        vx = __ldcg(S.vhat[0] + p);
+        vy = __ldcg(S.vhat[1] + p);
+        vz = __ldcg(S.vhat[2] + p);
+        vsc = __ldcg(S.vscale + p);
+        Ns = __ldcg(S.Nn[sp] + p);
+        if (s == 4) Ls = __ldcg(S.Ll[sp] + p);
+        if (s == 4 && sp == 0) t_in = __ldcg(S.time + p);
+#pragma unroll
+        for (int e = 0; e < NH; e++) y0[e] = s > 1 ? __ldcg(S.f0 + (sp * NH + e) * cap + p) : 0.0;
+        make_stencil<double>(P, x, y, z, st);
+    }
+    grid_dep_wait();
+    grid_dep_launch();
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+    zero_slice(mesh_zero, nzero);
+    if (active) {
         const double* __restrict__ fin = s == 1 ? S.f0 : S.fs;
-        const double vsc = S.vscale[p];
-        const double Ns = S.Nn[sp][p];
-        const double Ls = s == 4 ? S.Ll[sp][p] : 0.0;
-        const double t_in = (s == 4 && sp == 0) ? S.time[p] : 0.0;
-        double f[NH], y0[NH], a0[NH];
+        double f[NH], a0[NH];
 #pragma unroll
         for (int e = 0; e < NH; e++) {
             const long long o = (sp * NH + e) * cap + p;
             f[e] = fin[o];
-            y0[e] = s > 1 ? S.f0[o] : 0.0;
             a0[e] = s > 1 ? S.acc[o] : 0.0;
         }
-        make_stencil<double>(P, x, y, z, st);
         double V[NH], K[NH];
         potential_fp64_sp<NF, SWt>(P, mesh_in, st, vx, vy, vz, vsc, sp, V);
         commutator<NF, double>(V, f, K, P.inv_hbar);
@@ -665,12 +712,14 @@ __global__ void __launch_bounds__(2 * kBlock, 2) k_rk4_stage_split(DevParams P, 
                                                                   double* __restrict__ mesh_out, double* mesh_zero,
                                                                   long long nzero, StepCtl* ctl, int dt_mode)
 {
-    const int done = ctl->done;
-    const double dt = ctl->dt;
+    // stage 1 follows the previous step's last stage (or a re-sort), which
+    // writes the control block: it waits first
+    if (s == 1) grid_dep_wait();
+    const int done = __ldcg(&ctl->done);
+    const double dt = __ldcg(&ctl->dt);
     if (done) return;
     if (s == 1) record_dt(ctl, dt);
-    rk4_stage_body_split<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt);
-    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+    rk4_stage_body_split<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt, dt_mode);
 }
 
 template <int NF, int WX, int WY, int WZ>
@@ -678,14 +727,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S
                                                       double* __restrict__ mesh_out, double* mesh_zero, long long nzero,
                                                       StepCtl* ctl, int dt_mode)
 {
-    const int done = ctl->done;
-    const double dt = ctl->dt;   // both control loads in one round trip
+    if (s == 1) grid_dep_wait();   // (see k_rk4_stage_split)
+    const int done = __ldcg(&ctl->done);
+    const double dt = __ldcg(&ctl->dt);   // both control loads in one round trip
     if (done) return;
     if (s == 1) record_dt(ctl, dt);
-    rk4_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt);
-    // stage 4 of the device-resident loop: compute_dt on the stage-4 mesh
-    // (main.cpp:193-198), which this kernel only reads
-    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, mesh_in, ctl, DT_ADVANCE, reduce_blocks(P));
+    rk4_stage_body<NF, SW<WX, WY, WZ>>(P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt, dt_mode);
 }
 
 // Grid-wide barrier of the cooperative step kernel (its CTAs are co-resident
@@ -896,6 +943,8 @@ __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const lo
 {
     using H = Herm<NF>;
     constexpr int NH = NF * NF, ND = 8 * NH;
+    grid_dep_wait();   // the previous stage's deposit is complete
+    grid_dep_launch();
     if (ctl->done) return;
     zero_slice(qzero, qzero ? P.ncells * ND : 0);
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -979,46 +1028,67 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
     constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
-    const int done = ctl->done;
-    const double dt = ctl->dt;   // both control loads in one round trip
+    // (programmatic dependent launch: see grid_dep_wait; the finalize
+    // kernel before this stage has waited for the previous stage)
+    const int done = __ldcg(&ctl->done);
+    const double dt = __ldcg(&ctl->dt);   // both control loads in one round trip
     if (done) return;
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
     const long long cap = S.cap;
 
+    // prologue: fields that no kernel of this step writes (one memory round
+    // trip with the control loads; all of the state at the step start for
+    // two flavors in 1D, the per-species scalars otherwise)
     Stencil<float> st{};
     float fN[NS] = {};
     float vx = 0, vy = 0, vz = 0;
+    double x = 0, y = 0, z = 0, vs = 0, t_in = 0;
+    float Nsp[2] = {0.f, 0.f};
+    double Lsp[2] = {0, 0}, pu[4] = {0, 0, 0, 1};
+    const bool hoist = PRELOAD && s == 4;
+    constexpr int PRE = PRELOAD ? NS : 1;
+    double y0a[PRE];
+    float ka[PRE], ksa[PRE];
     if (active) {
-        const double x = S.pos[0][p], y = S.pos[1][p], z = S.pos[2][p];
-        vx = S.vhat32[0][p];
-        vy = S.vhat32[1][p];
-        vz = S.vhat32[2][p];
-        // the stage's per-particle loads are issued together (one memory
-        // round trip; all of the state for two flavors in 1D, the
-        // per-species scalars otherwise); the state arrays never alias
+        x = __ldcg(S.pos[0] + p);
+        y = __ldcg(S.pos[1] + p);
+        z = __ldcg(S.pos[2] + p);
+        vx = __ldcg(S.vhat32[0] + p);
+        vy = __ldcg(S.vhat32[1] + p);
+        vz = __ldcg(S.vhat32[2] + p);
+        vs = __ldcg(S.vscale + p);
+        Nsp[0] = __ldcg(S.N32[0] + p);
+        Nsp[1] = __ldcg(S.N32[1] + p);
+        if (hoist) {
+            Lsp[0] = __ldcg(S.Ll[0] + p);
+            Lsp[1] = __ldcg(S.Ll[1] + p);
+            t_in = __ldcg(S.time + p);
+#pragma unroll
+            for (int d = 0; d < 4; d++) pu[d] = __ldcg(S.pup[d] + p);
+        }
+        if constexpr (PRELOAD) {
+#pragma unroll
+            for (int c = 0; c < NS; c++) y0a[c] = __ldcg(S.f0 + c * cap + p);
+        }
+        make_stencil<float>(P, x, y, z, st);
+    }
+    grid_dep_wait();
+    grid_dep_launch();
+    // compute_dt on the stage-4 mesh (every block has read this step's dt)
+    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
+    if (active) {
+        // the state arrays never alias
         const double* __restrict__ f0p = S.f0;
         const float* __restrict__ k32p = S.k32;
         const float* __restrict__ ks32p = S.ksum32;
-        const double vs = S.vscale[p];
-        const float Nsp[2] = {S.N32[0][p], S.N32[1][p]};
-        const bool hoist = PRELOAD && s == 4;
-        const double Lsp[2] = {hoist ? S.Ll[0][p] : 0.0, hoist ? S.Ll[1][p] : 0.0};
-        const double t_in = hoist ? S.time[p] : 0.0;
-        const double pu[4] = {hoist ? S.pup[0][p] : 0.0, hoist ? S.pup[1][p] : 0.0, hoist ? S.pup[2][p] : 0.0,
-                              hoist ? S.pup[3][p] : 1.0};
-        constexpr int PRE = PRELOAD ? NS : 1;
-        double y0a[PRE];
-        float ka[PRE], ksa[PRE];
         if constexpr (PRELOAD) {
 #pragma unroll
             for (int c = 0; c < NS; c++) {
-                y0a[c] = f0p[c * cap + p];
                 ka[c] = s > 1 ? k32p[c * cap + p] : 0.f;
                 ksa[c] = s > 1 ? ks32p[c * cap + p] : 0.f;
             }
         }
-        make_stencil<float>(P, x, y, z, st);
         // FP32 self-interaction part, trace removed (it commutes)
         float hs[NH];
         potential_si32<NF, SWt>(P, gmesh, st, vx, vy, vz, hs);
@@ -1121,7 +1191,6 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         }
     }
     if (qout) tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4);
-    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
 }
 
 // ===========================================================================
@@ -1395,6 +1464,27 @@ void smem_optin(K kernel, int bytes)
     if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
+// launch with programmatic stream serialization: the kernel may start while
+// the previous kernel of the stream drains (the kernels launched this way
+// call grid_dep_wait before they read anything the previous kernel writes).
+// A launch error is left for cudaGetLastError, like a <<<>>> launch.
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                Args&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <int NF>
 void launch_rk4_stage_t(const DevParams& P, const DevState& S, int s, const double* mesh_in, double* mesh_out,
                         double* mesh_zero, long long nzero, StepCtl* ctl, int dt_mode, cudaStream_t st)
@@ -1403,12 +1493,12 @@ void launch_rk4_stage_t(const DevParams& P, const DevState& S, int s, const doub
         constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
         if constexpr (kSplit<NF, WXv, WYv>) {
             smem_optin(k_rk4_stage_split<NF, WXv, WYv, WZv>, bytes);
-            k_rk4_stage_split<NF, WXv, WYv, WZv><<<grid_for(S.n), 2 * kBlock, bytes, st>>>(
-                P, S, s, mesh_in, mesh_out, mesh_zero, nzero, ctl, dt_mode);
+            launch_pdl(k_rk4_stage_split<NF, WXv, WYv, WZv>, grid_for(S.n), 2 * kBlock, bytes, st, P, S, s, mesh_in,
+                       mesh_out, mesh_zero, nzero, ctl, dt_mode);
         } else {
             smem_optin(k_rk4_stage<NF, WXv, WYv, WZv>, bytes);
-            k_rk4_stage<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, s, mesh_in, mesh_out,
-                                                                                mesh_zero, nzero, ctl, dt_mode);
+            launch_pdl(k_rk4_stage<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock, bytes, st, P, S, s, mesh_in, mesh_out,
+                       mesh_zero, nzero, ctl, dt_mode);
         }
     });
 }
@@ -1496,8 +1586,9 @@ template <int NF>
 void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, const float* gmesh, long long* qout,
                               const long long* qdt, StepCtl* ctl, int dt_mode, cudaStream_t st)
 {
-    EMU_W_DISPATCH(P, (k_rk4_stage_mixed<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>(), st>>>(
-                          P, S, s, gmesh, qout, qdt, ctl, dt_mode)));
+    EMU_W_DISPATCH(P, (launch_pdl(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock,
+                                  tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>(), st, P, S, s, gmesh, qout, qdt,
+                                  ctl, dt_mode)));
 }
 
 template <int NF>
