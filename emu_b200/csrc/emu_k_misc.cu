@@ -147,8 +147,8 @@ static unsigned reduce_grid(long long ncells)
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
                            StepCtl* ctl, cudaStream_t st)
 {
-    EMU_NF_DISPATCH(nf, (launch_pdl(k_finalize_mixed<NFv>, reduce_grid(P.ncells), kBlock, 0, st, P, qread, qzero,
-                                    gmesh, ctl)));
+    EMU_NF_DISPATCH(nf, (launch_pdl(k_finalize_mixed<NFv>, reduce_grid(P.ncells * 4 * NFv * NFv), kBlock, 0, st, P,
+                                    qread, qzero, gmesh, ctl)));
 }
 
 void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st)

@@ -343,6 +343,79 @@ struct QuantConv {
     }
 };
 
+// Stable rank of the stencil keys held by the first NW warps of the block
+// (key -1 = inactive, ranked last): the permutation a stable radix sort of
+// the keys gives, by a counting sort over key - min(key) when the keys span
+// at most 31 consecutive values (a cell-sorted CTA whose particles moved a
+// few cells: the usual case).  Every thread of the block calls it; the
+// result is uniform over the block: false (nothing ranked, the caller sorts;
+// the scratch is free again) when the keys span more.  scratch: 2 NW + 32 NW
+// ints; on success it is read after the last barrier here, so the caller
+// waits at a barrier before it writes there.
+template <int NW>
+__device__ __forceinline__ bool small_range_rank(int key, int* scratch, int& slot)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool part = w < NW;
+    int* red = scratch;            // per-warp min (NW) and max (NW) of the active keys
+    int* cnt = scratch + 2 * NW;   // [warp][bucket] counts, then bases
+    if (part) {
+        const unsigned mn = __reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0xffffffffu);
+        const unsigned mx = __reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
+        if (lane == 0) {
+            red[w] = (int)mn;
+            red[NW + w] = (int)mx;
+        }
+        cnt[w * 32 + lane] = 0;
+    }
+    __syncthreads();
+    unsigned kmin = 0xffffffffu, kmax = 0u;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+        kmin = min(kmin, (unsigned)red[i]);
+        kmax = max(kmax, (unsigned)red[NW + i]);
+    }
+    const int range = kmin == 0xffffffffu ? 0 : (int)(kmax - kmin) + 1;   // inactive bucket = range
+    if (range > 31) {
+        // every thread has read red[] before the caller's sort reuses the scratch
+        __syncthreads();
+        return false;
+    }
+    int d = 0, rank = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    if (part) {
+        d = key >= 0 ? (int)((unsigned)key - kmin) : range;
+        const unsigned peers = __match_any_sync(kFull, d);
+        rank = __popc(peers & lt);
+        if ((peers & lt) == 0u) cnt[w * 32 + d] = __popc(peers);
+    }
+    __syncthreads();
+    if (w == 0) {
+        // lane = bucket: base of each (bucket, warp) in bucket-major order
+        int c[NW], tot = 0;
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+            c[i] = cnt[i * 32 + lane];
+            tot += c[i];
+        }
+        int inc = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, inc, o);
+            if (lane >= o) inc += t;
+        }
+        int base = inc - tot;
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+            cnt[i * 32 + lane] = base;
+            base += c[i];
+        }
+    }
+    __syncthreads();
+    if (part) slot = cnt[w * 32 + d] + rank;
+    return true;
+}
+
 // sort_keys: the CTA's particles are not in stencil order (the deposit of
 // moved particles at the end of a step): the 128 keys are radix-sorted in
 // shared memory first, so that each stencil forms one run
@@ -360,15 +433,19 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
     const int key = active ? stencil_key(P, st.b) : -1;
     int slot = threadIdx.x;
     if (sort_keys) {
-        // sort the keys (scratch in the record area, not yet written), then
+        // rank the keys (scratch in the record area, not yet written), then
         // every thread writes its record at its key's rank
-        auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
-        unsigned k[1] = {key >= 0 ? (unsigned)key : (unsigned)P.ncells};   // inactive slots last
-        int v[1] = {(int)threadIdx.x};
-        Sort(tmp).Sort(k, v, 0, P.key_bits);
-        srank[v[0]] = threadIdx.x;
-        __syncthreads();
-        slot = srank[threadIdx.x];
+        if (small_range_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), slot)) {
+            __syncthreads();   // (the record area held the ranking scratch)
+        } else {
+            auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
+            unsigned k[1] = {key >= 0 ? (unsigned)key : (unsigned)P.ncells};   // inactive slots last
+            int v[1] = {(int)threadIdx.x};
+            Sort(tmp).Sort(k, v, 0, P.key_bits);
+            srank[v[0]] = threadIdx.x;
+            __syncthreads();
+            slot = srank[threadIdx.x];
+        }
     }
     tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
     __syncthreads();
@@ -396,12 +473,18 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
     const int key = active ? stencil_key(P, st.b) : -1;
     int slot = pl;
     if (sort_keys) {
-        // species-1 threads sort behind every real key (ncells + 1)
-        auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
-        unsigned k[1] = {sp ? (unsigned)P.ncells + 1u : (key >= 0 ? (unsigned)key : (unsigned)P.ncells)};
-        int v[1] = {(int)threadIdx.x};
-        Sort(tmp).Sort(k, v, 0, P.key_bits + 1);
-        if (threadIdx.x < kBlock) srank[v[0]] = threadIdx.x;
+        int sl = pl;
+        if (small_range_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), sl)) {
+            // the species-0 threads (the first kBlock) hold the ranks
+            if (sp == 0) srank[pl] = sl;
+        } else {
+            // species-1 threads sort behind every real key (ncells + 1)
+            auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
+            unsigned k[1] = {sp ? (unsigned)P.ncells + 1u : (key >= 0 ? (unsigned)key : (unsigned)P.ncells)};
+            int v[1] = {(int)threadIdx.x};
+            Sort(tmp).Sort(k, v, 0, P.key_bits + 1);
+            if (threadIdx.x < kBlock) srank[v[0]] = threadIdx.x;
+        }
         __syncthreads();
         slot = srank[pl];
     }
@@ -935,30 +1018,30 @@ __global__ void __launch_bounds__(kBlock) k_dt(DevParams P, const T* __restrict_
 // ===========================================================================
 // finalize an int64 mesh into FP32 potentials G[cell][d][e] =
 // sqrt(2)GF/dV * (M_d,nu,e + sgn_e M_d,nubar,e) and zero the other int64
-// mesh (the one the next stage deposits into).
+// mesh (the one the next stage deposits into).  One thread per output value
+// (cell-major, coalesced): a cell per thread left a 1024-cell mesh on 8 SMs.
 template <int NF>
 __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const long long* __restrict__ q,
                                                            long long* __restrict__ qzero, float* __restrict__ g,
                                                            StepCtl* ctl)
 {
     using H = Herm<NF>;
-    constexpr int NH = NF * NF, ND = 8 * NH;
+    constexpr int NH = NF * NF, ND = 8 * NH, NG = 4 * NH;
     grid_dep_wait();   // the previous stage's deposit is complete
     grid_dep_launch();
     if (ctl->done) return;
     zero_slice(qzero, qzero ? P.ncells * ND : 0);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.ncells; c += stride) {
+    const long long total = P.ncells * NG;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long c = i / NG;
+        const int k = (int)(i - c * NG);
+        const int d = k / NH, e = k - d * NH;
         const long long* m = q + c * ND;
-#pragma unroll
-        for (int d = 0; d < 4; d++)
-#pragma unroll
-            for (int e = 0; e < NH; e++) {
-                const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
-                const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
-                const double comb = H::is_im(e) ? a + b : a - b;
-                g[c * 4 * NH + d * NH + e] = (float)(P.sqrt2GF_inv_vol * comb);
-            }
+        const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
+        const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
+        const double comb = H::is_im(e) ? a + b : a - b;
+        g[i] = (float)(P.sqrt2GF_inv_vol * comb);
     }
 }
 

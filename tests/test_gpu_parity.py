@@ -113,6 +113,29 @@ def test_evolve_3d_matches_oracle():
     assert colwise_rel(out[:, flavor_cols(3)], ref[:, flavor_cols(3)]) < 1e-11
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_evolve_3d_wide_tiles_match_oracle(mixed):
+    """3D TSC with two particles per cell and no re-sort: the stencil keys of
+    a CTA's 128 particles span ~64 cells, so the load deposit and every
+    stage-4 deposit of moved particles rank them with the block radix sort
+    (the counting sort covers spans of at most 31 cells)"""
+    p = W.c5_3d(n=6, ndirs=2, mixed=mixed)
+    p.resort_interval = 0
+    parts = api.init_particles(p)
+    o = Oracle(p)
+    ref, t_ref, _, _ = o.evolve(parts, 4)
+    with api.Context(p) as c:
+        c.load_particles(parts)
+        info = c.evolve(4)
+        assert info.status == 0 and info.steps_done == 4
+        out = c.get_particles()
+    fc = flavor_cols(3)
+    if mixed:   # (a wrong rank would misplace whole records: O(1) errors)
+        assert colwise_rel(out[:, fc], ref[:, fc]) < 1e-4
+    else:
+        assert colwise_rel(out, ref) < 1e-11
+
+
 def test_evolve_end_time_clipping():
     p = _c2_small(ncz=8, ndirs=6)
     parts = api.init_particles(p)
