@@ -248,7 +248,7 @@ def run_emu(args):
     # the library's automatic re-sort interval (resort_interval < 0)
     eff_resort = p.resort_interval
     if eff_resort < 0:
-        eff_resort = 1 if sum(1 for c in p.ncell if c > 1) == 3 and p.shape_order >= 2 else 4
+        eff_resort = 1 if sum(1 for c in p.ncell if c > 1) == 3 and p.shape_order >= 2 else 16
     total_steps = args.warmup + args.steps + args.profile_steps + 8
     ctx.evolve_begin(0.0, float("inf"), total_steps)
     flush_bytes = 512 << 20

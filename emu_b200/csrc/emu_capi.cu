@@ -544,8 +544,11 @@ int emu_create(const emu_params* p, emu_context** out)
         // step or two once particles leave their cells, a 1D stencil within
         // several
         const int cells = ctx->P.w[0] * ctx->P.w[1] * ctx->P.w[2];
-        ctx->prm.resort_interval = cells > 9 ? 1 : 4;
+        ctx->prm.resort_interval = cells > 9 ? 1 : 16;
     }
+    // with a re-sort after every step, the deposits of stages 1-3 see
+    // cell-sorted particles; otherwise every deposit ranks its keys
+    ctx->P.rank_stages = ctx->prm.resort_interval != 1;
     int r = EMU_OK;
     auto bail = [&](int code) {
         g_host_err = ctx->err;

@@ -59,6 +59,7 @@ struct DevParams {
     int ord[3];        // shape order per dimension
     long long ncells;
     int key_bits;      // bits of a stencil key in [0, ncells]
+    int rank_stages;   // particles may have moved since the last re-sort: every deposit ranks its keys
     double L[3];       // domain length (periodic, [0,L))
     double dxi[3];     // inverse cell size
     double sqrt2GF_inv_vol;   // sqrt(2)*GF*inv_cell_volume (Evolve.cpp:167 + fill)

@@ -344,50 +344,74 @@ struct QuantConv {
 };
 
 // Stable rank of the stencil keys held by the first NW warps of the block
-// (key -1 = inactive, ranked last): the permutation a stable radix sort of
-// the keys gives, by a counting sort over key - min(key) when the keys span
-// at most 31 consecutive values (a cell-sorted CTA whose particles moved a
-// few cells: the usual case).  Every thread of the block calls it; the
-// result is uniform over the block: false (nothing ranked, the caller sorts;
-// the scratch is free again) when the keys span more.  scratch: 2 NW + 32 NW
-// ints; on success it is read after the last barrier here, so the caller
-// waits at a barrier before it writes there.
+// (key -1 = inactive, ranked last): the permutation a stable sort of the
+// keys gives, by a counting sort over the distinct keys when the warps hold
+// at most 32 (warp, key) groups (cell-sorted particles that moved a few
+// cells: the usual case).  Group leaders list their keys, one warp sorts the
+// list (bitonic, shuffles) and drops repeats, every thread finds its key's
+// bucket by binary search, and one warp scans the (bucket, warp) counts.
+// Every thread of the block calls it; the result is uniform over the block:
+// false (nothing ranked, the caller sorts; the scratch is free again) when
+// there are more groups.  scratch: 66 + 32 NW ints; on success it is read
+// after the last barrier here, so the caller waits at a barrier before it
+// writes there.
 template <int NW>
-__device__ __forceinline__ bool small_range_rank(int key, int* scratch, int& slot)
+__device__ __forceinline__ bool distinct_key_rank(int key, int* scratch, int& slot)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const bool part = w < NW;
-    int* red = scratch;            // per-warp min (NW) and max (NW) of the active keys
-    int* cnt = scratch + 2 * NW;   // [warp][bucket] counts, then bases
+    const unsigned lt = (1u << lane) - 1u;
+    int* ngroups = scratch;                                      // (warp, key) groups listed
+    int* nkeys = scratch + 1;                                    // distinct keys
+    unsigned* list = reinterpret_cast<unsigned*>(scratch + 2);   // [32] group keys
+    unsigned* ukey = list + 32;                                  // [32] sorted distinct keys
+    int* cnt = scratch + 66;                                     // [NW][32] counts, then bases
+    if (threadIdx.x == 0) *ngroups = 0;
+    if (part) cnt[w * 32 + lane] = 0;
+    __syncthreads();
+    const unsigned k = key >= 0 ? (unsigned)key : 0xffffffffu;   // inactive last
+    unsigned peers = 0u;
     if (part) {
-        const unsigned mn = __reduce_min_sync(kFull, key >= 0 ? (unsigned)key : 0xffffffffu);
-        const unsigned mx = __reduce_max_sync(kFull, key >= 0 ? (unsigned)key : 0u);
-        if (lane == 0) {
-            red[w] = (int)mn;
-            red[NW + w] = (int)mx;
+        peers = __match_any_sync(kFull, k);
+        if ((peers & lt) == 0u) {
+            const int i = atomicAdd(ngroups, 1);
+            if (i < 32) list[i] = k;
         }
-        cnt[w * 32 + lane] = 0;
     }
     __syncthreads();
-    unsigned kmin = 0xffffffffu, kmax = 0u;
-#pragma unroll
-    for (int i = 0; i < NW; i++) {
-        kmin = min(kmin, (unsigned)red[i]);
-        kmax = max(kmax, (unsigned)red[NW + i]);
-    }
-    const int range = kmin == 0xffffffffu ? 0 : (int)(kmax - kmin) + 1;   // inactive bucket = range
-    if (range > 31) {
-        // every thread has read red[] before the caller's sort reuses the scratch
-        __syncthreads();
+    const int ng = *ngroups;
+    if (ng > 32) {
+        __syncthreads();   // every thread has read the count before the caller's sort reuses the scratch
         return false;
     }
-    int d = 0, rank = 0;
-    const unsigned lt = (1u << lane) - 1u;
+    if (w == 0) {
+        unsigned v = lane < ng ? list[lane] : 0xffffffffu;
+#pragma unroll
+        for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                const unsigned o = __shfl_xor_sync(kFull, v, stride);
+                const bool up = (lane & size) == 0, lower = (lane & stride) == 0;
+                v = (lower == up) ? min(v, o) : max(v, o);
+            }
+        const unsigned prev = __shfl_up_sync(kFull, v, 1);
+        const bool first = lane == 0 || prev != v;
+        const unsigned fm = __ballot_sync(kFull, first);
+        if (first) ukey[__popc(fm & lt)] = v;
+        if (lane == 0) *nkeys = __popc(fm);
+    }
+    __syncthreads();
+    int b = 0, rank = 0;
     if (part) {
-        d = key >= 0 ? (int)((unsigned)key - kmin) : range;
-        const unsigned peers = __match_any_sync(kFull, d);
+        int lo = 0, hi = *nkeys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (ukey[mid] < k) lo = mid + 1;
+            else hi = mid;
+        }
+        b = lo;
         rank = __popc(peers & lt);
-        if ((peers & lt) == 0u) cnt[w * 32 + d] = __popc(peers);
+        if ((peers & lt) == 0u) cnt[w * 32 + b] = __popc(peers);
     }
     __syncthreads();
     if (w == 0) {
@@ -412,13 +436,14 @@ __device__ __forceinline__ bool small_range_rank(int key, int* scratch, int& slo
         }
     }
     __syncthreads();
-    if (part) slot = cnt[w * 32 + d] + rank;
+    if (part) slot = cnt[w * 32 + b] + rank;
     return true;
 }
 
-// sort_keys: the CTA's particles are not in stencil order (the deposit of
-// moved particles at the end of a step): the 128 keys are radix-sorted in
-// shared memory first, so that each stencil forms one run
+// sort_keys: the CTA's particles may not be in stencil order (particles
+// that moved since the last re-sort; the deposit of moved particles at the
+// end of a step): the 128 keys are ranked first (stable, so cell-sorted
+// particles keep their order), so that each stencil forms one run
 template <int NF, class SWt, class R, class T, class Conv>
 __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
                                                    const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false)
@@ -426,6 +451,8 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
     using Sort = cub::BlockRadixSort<unsigned, kBlock, 1, int>;
     static_assert(sizeof(typename Sort::TempStorage) <= kBlock * TileRec<NF, SWt, R>::RW * sizeof(R),
                   "sort scratch aliases the record area");
+    static_assert((66 + kBlock) * sizeof(int) <= kBlock * TileRec<NF, SWt, R>::RW * sizeof(R),
+                  "rank scratch aliases the record area");
     extern __shared__ __align__(16) unsigned char tile_smem[];
     int* skey = reinterpret_cast<int*>(tile_smem);
     int* srank = skey + kBlock;
@@ -435,7 +462,7 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
     if (sort_keys) {
         // rank the keys (scratch in the record area, not yet written), then
         // every thread writes its record at its key's rank
-        if (small_range_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), slot)) {
+        if (distinct_key_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), slot)) {
             __syncthreads();   // (the record area held the ranking scratch)
         } else {
             auto& tmp = *reinterpret_cast<typename Sort::TempStorage*>(srec);
@@ -465,6 +492,7 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
     constexpr int NT = 2 * kBlock, NH = NF * NF, RW = TR::RW, SP = TR::SP;
     using Sort = cub::BlockRadixSort<unsigned, NT, 1, int>;
     static_assert(sizeof(typename Sort::TempStorage) <= kBlock * RW * sizeof(R), "sort scratch aliases the records");
+    static_assert((66 + kBlock) * sizeof(int) <= kBlock * RW * sizeof(R), "rank scratch aliases the records");
     extern __shared__ __align__(16) unsigned char tile_smem[];
     int* skey = reinterpret_cast<int*>(tile_smem);
     int* srank = skey + kBlock;
@@ -474,7 +502,7 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
     int slot = pl;
     if (sort_keys) {
         int sl = pl;
-        if (small_range_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), sl)) {
+        if (distinct_key_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), sl)) {
             // the species-0 threads (the first kBlock) hold the ranks
             if (sp == 0) srank[pl] = sl;
         } else {
@@ -653,7 +681,7 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
     }
     if (mesh_out)   // (null: the stage-4 deposit is made by the re-sort gather)
         tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
-                                            [](double a, int) -> double { return a; }, s == 4);
+                                            [](double a, int) -> double { return a; }, s == 4 || P.rank_stages);
 }
 
 // FP64 potential of one species (potential_fp64 restricted to species sp)
@@ -780,7 +808,7 @@ __device__ __forceinline__ void rk4_stage_body_split(const DevParams& P, const D
     }
     if (mesh_out)
         tile_deposit_block_split<NF, SWt, double>(P, mesh_out, active, st, sp, fN, vx, vy, vz,
-                                                  [](double a, int) -> double { return a; }, s == 4);
+                                                  [](double a, int) -> double { return a; }, s == 4 || P.rank_stages);
 }
 
 // Two flavors, 1D stencils: species-split kernels (2 kBlock threads per
@@ -1273,7 +1301,8 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
             make_stencil<float>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    if (qout) tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4);
+    if (qout)
+        tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4 || P.rank_stages);
 }
 
 // ===========================================================================

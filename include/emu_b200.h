@@ -104,7 +104,7 @@ typedef struct emu_params {
                                 (the reference seeds from the clock, main.cpp:240) */
     int resort_interval;     /* steps between on-device cell re-sorts (0 = never,
                                 < 0 = automatic: every step for 3D stencils,
-                                every 4 steps otherwise; default -1) */
+                                every 16 steps otherwise; default -1) */
     int fused;               /* RK4 kernels: 1 (default) one fused kernel per stage, a CUDA
                                 graph per step; 2: one cooperative launch per step when the
                                 grid fits on the GPU at once (FP64), else as 1; 0: unfused */
