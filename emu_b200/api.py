@@ -136,6 +136,9 @@ SIGNATURES = {
     "emu_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D,
                                            _P(EmuRunInfo)]),
     "emu_adjoint_objective": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
+    "emu_adjoint_reserve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int)]),
     "emu_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _D]),
 }
 
@@ -369,6 +372,14 @@ class Context:
         self._ck(self.lib.emu_attach_comm(self.h, comm_id, int(rank), int(nranks)), "emu_attach_comm")
 
     # ---- discrete adjoint (FP64 RK4) ----
+    def adjoint_reserve(self, nsteps, checkpoint_interval):
+        """Allocate a recorded run's storage up front; returns (device bytes,
+        stage states stored per segment, sub-checkpoint spacing or 0)."""
+        b, st, sub = ctypes.c_int64(0), ctypes.c_int(0), ctypes.c_int(0)
+        self._ck(self.lib.emu_adjoint_reserve(self.h, int(nsteps), int(checkpoint_interval), ctypes.byref(b),
+                                              ctypes.byref(st), ctypes.byref(sub)), "emu_adjoint_reserve")
+        return int(b.value), bool(st.value), int(sub.value)
+
     def adjoint_forward(self, nsteps, checkpoint_interval, start_time=0.0):
         """Recorded run of nsteps from the loaded state; returns (dts, info)."""
         dts = np.zeros(int(nsteps))

@@ -49,13 +49,15 @@ struct emu_adjoint {
     int nsteps = 0, interval = 0, nck = 0;
     bool recorded = false;
     bool store = false;         // stage states of a whole segment fit (else one step at a time)
+    int sub = 0;                // per-step mode: sub-checkpoint spacing inside a segment (0: none)
     double t0 = 0.0;
     std::vector<double> dts;
     std::vector<char> resorted; // segment c began with a cell re-sort (permutation perm[c])
     double* dts_dev = nullptr;
     double* ck = nullptr;       // nck x (NS + 3) x cap: Y_0 then x, y, z per checkpoint
     unsigned* perm = nullptr;   // nck x cap gather permutations of the segment-start re-sorts
-    double* seg = nullptr;      // interval x (NS + 3) x cap: Y_0, x of every step of a segment
+    double* seg = nullptr;      // seg_slots x (NS + 3) x cap: Y_0, x of every step of a segment
+                                // (with sub-checkpoints: of a sub-segment, then the sub-checkpoints)
     double* sst = nullptr;      // stored stage states (4 x NS x cap per step)
     double* mst = nullptr;      // stored meshes M_1..M_4 per step
     double* stat = nullptr;     // two working copies of the static particle fields
@@ -63,6 +65,8 @@ struct emu_adjoint {
     double* lmesh[4] = {};      // adjoint meshes (rotating)
     double* nex = nullptr;      // ncells x 2 objective components
     long long seg_slots = 0, ck_slots = 0;
+    int interval_cap = 0;       // longest segment the slots serve
+    size_t bytes = 0;           // device memory held
     double *acc = nullptr, *lamY0 = nullptr, *lamN = nullptr, *lamn = nullptr, *lamYd = nullptr;
     double *wf = nullptr, *lamtmp = nullptr, *wpos = nullptr, *wtime = nullptr;
     double* rows = nullptr;     // n x NS staging for host transfers
@@ -579,7 +583,7 @@ __global__ void k_seg_save(DevState R, double* __restrict__ slot, int NS, const 
 {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p == 0 && ctl) ctl->dt = dts[k];
-    if (p >= R.n) return;
+    if (p >= R.n || !slot) return;   // (no slot: only the dt of step k)
     const long long cap = R.cap;
     for (int c = 0; c < NS; c++) slot[c * cap + p] = R.f0[c * cap + p];
     for (int d = 0; d < 3; d++) slot[(NS + d) * cap + p] = R.pos[d][p];
@@ -856,7 +860,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
     const int nck = (nsteps + interval - 1) / interval;
     const long long nm = mesh_elems(ctx);
     emu_adjoint* a = ctx->adj;
-    if (a && (a->cap != cap || a->NS != NS || a->ck_slots < nck || a->seg_slots < interval ||
+    if (a && (a->cap != cap || a->NS != NS || a->ck_slots < nck || a->interval_cap < interval ||
               (int)a->dts.size() < nsteps)) {
         free_adj(a);
         a = ctx->adj = nullptr;
@@ -868,7 +872,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         a->NS = NS;
         a->dts.resize(std::max(nsteps, 1));
         a->ck_slots = std::max(nck, 1);
-        a->seg_slots = interval;
+        a->interval_cap = interval;
         a->resorted.assign(a->ck_slots, 0);
         const size_t slot = (size_t)(NS + 3) * cap;
         // stage states and meshes of every step of a segment when they take
@@ -881,18 +885,42 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         const size_t per_step = sizeof(double) * ((size_t)4 * NS * cap + (size_t)4 * nm);
         a->store = (size_t)interval * per_step <= budget;
         const size_t st_steps = a->store ? (size_t)interval : 1;
-        CU(cudaMalloc(&a->dts_dev, sizeof(double) * a->dts.size()));
-        CU(cudaMalloc(&a->ck, sizeof(double) * slot * a->ck_slots));
-        CU(cudaMalloc(&a->seg, sizeof(double) * slot * a->seg_slots));
-        CU(cudaMalloc(&a->perm, sizeof(unsigned) * cap * a->ck_slots));
-        CU(cudaMalloc(&a->stat, (size_t)2 * 13 * 8 * cap));
-        CU(cudaMalloc(&a->sst, sizeof(double) * st_steps * 4 * NS * cap));
-        CU(cudaMalloc(&a->mst, sizeof(double) * st_steps * 4 * nm));
+        // per-step mode: the states of every step of a segment (interval
+        // slots), or, when the checkpoints and those slots would not fit in
+        // the free memory, sub-checkpoints every J ~ sqrt(interval) steps
+        // (J + interval / J slots; each step is recomputed once more)
+        a->sub = 0;
+        a->seg_slots = interval;
+        if (!a->store) {
+            const size_t other = sizeof(double) * ((size_t)st_steps * 4 * (NS * cap + nm) + (size_t)(6 * NS + 8) * cap +
+                                                   (size_t)4 * nm + (size_t)NS * cap + 2 * 13 * cap) +
+                                 sizeof(unsigned) * (size_t)cap * a->ck_slots;
+            const size_t single = sizeof(double) * slot * (size_t)(a->ck_slots + interval) + other;
+            int J = 0;
+            if (single > fre / 20 * 19) J = (int)std::ceil(std::sqrt((double)interval));
+            if (const char* env = std::getenv("EMU_ADJOINT_SUBCHECKPOINT")) J = std::atoi(env);
+            if (J > 0 && J < interval) {
+                a->sub = J;
+                a->seg_slots = J + (interval + J - 1) / J;
+            }
+        }
+        a->bytes = 0;
+        auto alloc = [&](auto** ptr, size_t b) {
+            a->bytes += b;
+            return cudaMalloc(reinterpret_cast<void**>(ptr), b);
+        };
+        CU(alloc(&a->dts_dev, sizeof(double) * a->dts.size()));
+        CU(alloc(&a->ck, sizeof(double) * slot * a->ck_slots));
+        CU(alloc(&a->seg, sizeof(double) * slot * a->seg_slots));
+        CU(alloc(&a->perm, sizeof(unsigned) * cap * a->ck_slots));
+        CU(alloc(&a->stat, (size_t)2 * 13 * 8 * cap));
+        CU(alloc(&a->sst, sizeof(double) * st_steps * 4 * NS * cap));
+        CU(alloc(&a->mst, sizeof(double) * st_steps * 4 * nm));
         // acc, lamY0, lamn, lamYd, wf, lamtmp: 6 NS; lamN 2, lamtmp 2; wpos 3; wtime 1
-        CU(cudaMalloc(&a->work, sizeof(double) * (size_t)(6 * NS + 8) * cap));
-        for (int i = 0; i < 4; i++) CU(cudaMalloc(&a->lmesh[i], sizeof(double) * nm));
-        CU(cudaMalloc(&a->nex, sizeof(double) * 2 * ctx->P.ncells));
-        CU(cudaMalloc(&a->rows, sizeof(double) * (size_t)NS * cap));
+        CU(alloc(&a->work, sizeof(double) * (size_t)(6 * NS + 8) * cap));
+        for (int i = 0; i < 4; i++) CU(alloc(&a->lmesh[i], sizeof(double) * nm));
+        CU(alloc(&a->nex, sizeof(double) * 2 * ctx->P.ncells));
+        CU(alloc(&a->rows, sizeof(double) * (size_t)NS * cap));
         double* w = a->work;
         a->acc = w; w += (size_t)NS * cap;
         a->lamY0 = w; w += (size_t)NS * cap;
@@ -987,6 +1015,22 @@ void emu_ctx::adjoint_free(emu_context* ctx)
         free_adj(ctx->adj);
         ctx->adj = nullptr;
     }
+}
+
+int emu_adjoint_reserve(emu_context* ctx, int nsteps, int checkpoint_interval, int64_t* device_bytes,
+                        int* stage_store, int* sub_interval)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    int r;
+    if ((r = check_ready(ctx, "emu_adjoint_reserve"))) return r;
+    if (nsteps < 1 || checkpoint_interval < 1)
+        return fail(ctx, EMU_ERR_ARG, "emu_adjoint_reserve: nsteps and checkpoint_interval must be >= 1");
+    if ((r = ensure_adj(ctx, nsteps, checkpoint_interval))) return r;
+    const emu_adjoint* a = ctx->adj;
+    if (device_bytes) *device_bytes = (int64_t)a->bytes;
+    if (stage_store) *stage_store = a->store ? 1 : 0;
+    if (sub_interval) *sub_interval = a->sub;
+    return EMU_OK;
 }
 
 int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, double start_time, double* dts,
@@ -1144,31 +1188,57 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
             CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * (size_t)len * 4 * nm, st));
             if ((r = segment_sweep(ctx, W, G, coop))) return r;
         } else {
-            // (Y_0, x) of every step of the segment, then each step as a
+            // (Y_0, x) of every step of a sub-segment (the whole segment
+            // unless memory asked for sub-checkpoints), recomputed from the
+            // segment checkpoint or a sub-checkpoint, then each step as a
             // one-step segment (its stage states recomputed)
             DevState R = W;
             R.f0 = a->wf;
             for (int d = 0; d < 3; d++) R.pos[d] = a->wpos + (size_t)d * cap;
             R.time = a->wtime;
             double* const* M = ctx->mesh;
-            CU(cudaMemcpyAsync(a->wf, slot_f(a, a->ck, seg), sizeof(double) * NS * cap, cudaMemcpyDeviceToDevice, st));
-            CU(cudaMemcpyAsync(a->wpos, slot_x(a, a->ck, seg, 0), sizeof(double) * 3 * cap, cudaMemcpyDeviceToDevice,
-                               st));
-            CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
-            if ((r = deposit_into(ctx, R, R.f0, M[0]))) return r;
-            for (int k = k0; k < k1; k++) {
-                emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(R, slot_f(a, a->seg, k - k0), NS, a->dts_dev, k, ctx->ctl);
-                if (k + 1 == k1) break;
+            const int J = (a->sub > 0 && a->sub < len) ? a->sub : len;   // steps per sub-segment
+            const int nsub = (len + J - 1) / J;
+            // sub-checkpoint i >= 1 (state at step k0 + i J) sits in seg slot J + i
+            auto restore = [&](const double* slot) -> int {
+                CU(cudaMemcpyAsync(a->wf, slot, sizeof(double) * NS * cap, cudaMemcpyDeviceToDevice, st));
+                CU(cudaMemcpyAsync(a->wpos, slot + (size_t)NS * cap, sizeof(double) * 3 * cap,
+                                   cudaMemcpyDeviceToDevice, st));
+                CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
+                return deposit_into(ctx, R, R.f0, M[0]);
+            };
+            auto advance = [&]() {
                 for (int s = 1; s <= 4; s++)
                     emu::launch_rk4_stage(nf, ctx->P, R, s, M[s - 1], M[s % 4], M[(s + 1) % 4], nm, ctx->ctl, -1, st);
+            };
+            if (nsub > 1) {
+                if ((r = restore(slot_f(a, a->ck, seg)))) return r;
+                const int kl = k0 + (nsub - 1) * J;
+                for (int k = k0; k <= kl; k++) {
+                    const bool save = k > k0 && (k - k0) % J == 0;
+                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(
+                        R, save ? slot_f(a, a->seg, J + (k - k0) / J) : nullptr, NS, a->dts_dev, k, ctx->ctl);
+                    if (k < kl) advance();
+                }
+                if ((r = check_launch(ctx, "adjoint sub-checkpoints"))) return r;
             }
-            if ((r = check_launch(ctx, "adjoint segment recompute"))) return r;
-            for (int k = k1 - 1; k >= k0; k--) {
-                G.seg = slot_f(a, a->seg, k - k0);
-                G.k0 = k;
-                G.len = 1;
-                CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * 4 * nm, st));
-                if ((r = segment_sweep(ctx, W, G, false))) return r;
+            for (int i = nsub - 1; i >= 0; i--) {
+                const int s0 = k0 + i * J, s1 = std::min(s0 + J, k1);
+                if ((r = restore(i == 0 ? slot_f(a, a->ck, seg) : slot_f(a, a->seg, J + i)))) return r;
+                for (int k = s0; k < s1; k++) {
+                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(R, slot_f(a, a->seg, k - s0), NS, a->dts_dev, k,
+                                                                ctx->ctl);
+                    if (k + 1 == s1) break;
+                    advance();
+                }
+                if ((r = check_launch(ctx, "adjoint segment recompute"))) return r;
+                for (int k = s1 - 1; k >= s0; k--) {
+                    G.seg = slot_f(a, a->seg, k - s0);
+                    G.k0 = k;
+                    G.len = 1;
+                    CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * 4 * nm, st));
+                    if ((r = segment_sweep(ctx, W, G, false))) return r;
+                }
             }
         }
         if (seg > 0 && a->resorted[seg]) {

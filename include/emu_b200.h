@@ -270,8 +270,20 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * states and meshes of a whole segment are kept when they fit a budget
  * (a quarter of the free device memory, at most 16 GiB; environment variable
  * EMU_ADJOINT_STORE_MAX_BYTES overrides it), else each step's stages are
- * recomputed before its backward step.  The context's particle state is
+ * recomputed before its backward step.  In that per-step mode the states of
+ * every step of a segment are kept, or, when the checkpoints and those
+ * states would not fit in the free device memory, sub-checkpoints every
+ * J = ceil(sqrt(checkpoint_interval)) steps (J + interval / J states; each
+ * step is recomputed once more; environment variable
+ * EMU_ADJOINT_SUBCHECKPOINT sets J).  The context's particle state is
  * unchanged.
+ *
+ * emu_adjoint_reserve: allocates the checkpoint and work storage of a
+ * recorded run of nsteps with this checkpoint_interval up front (what
+ * emu_adjoint_forward would allocate), so that a timed or repeated run does
+ * no allocation.  Optional outputs: the device bytes held, whether stage
+ * states of whole segments are stored (1) or recomputed per step (0), and
+ * the sub-checkpoint spacing (0 = none).
  */
 /*
  * Particle sharding over GPUs (one process per GPU).  No counterpart in the
@@ -299,6 +311,8 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
 int emu_adjoint_objective(emu_context* ctx, double* J, double* lam_f, double* lam_N);
 int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const double* lam_N_final, double* lam_f0,
                          double* lam_N0);
+int emu_adjoint_reserve(emu_context* ctx, int nsteps, int checkpoint_interval, int64_t* device_bytes,
+                        int* stage_store, int* sub_interval);
 
 #ifdef __cplusplus
 }

@@ -151,16 +151,20 @@ def test_adjoint_errors():
             c.adjoint_forward(3, 2)
 
 
-@pytest.mark.parametrize("store", ["segment", "per_step"])
+@pytest.mark.parametrize("store", ["segment", "per_step", "per_step_sub2", "per_step_sub3"])
 def test_adjoint_memory_modes_agree(monkeypatch, store):
-    """stage states kept for a whole segment, or recomputed step by step
-    (budget 0): same gradient to rounding"""
-    if store == "per_step":
+    """stage states kept for a whole segment, recomputed step by step
+    (budget 0), or step by step from sub-checkpoints every 2 or 3 steps
+    inside a 7-step segment (the mode for runs whose checkpoints and step
+    states would not fit in memory): same gradient to rounding"""
+    if store != "segment":
         monkeypatch.setenv("EMU_ADJOINT_STORE_MAX_BYTES", "0")
+    if store.startswith("per_step_sub"):
+        monkeypatch.setenv("EMU_ADJOINT_SUBCHECKPOINT", store[-1])
     p = W.c2_fast_flavor_1d(ncell_z=8, ndirs=6)
     parts = api.init_particles(p)
     fc, nc = flavor_columns(2), number_columns(2)
-    with AdjointRun(p, parts, 7, 3) as run:
+    with AdjointRun(p, parts, 16, 7) as run:
         run.forward(parts[:, fc], parts[:, nc])
         J, lf, lN = run.ctx.adjoint_objective()
         g, gN = run.ctx.adjoint_backward(lf, lN)
