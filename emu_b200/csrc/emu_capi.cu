@@ -610,6 +610,8 @@ void emu_destroy(emu_context* ctx)
     if (ctx->aos) cudaFree(ctx->aos);
     if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
     if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
+    if (ctx->stats) cudaFree(ctx->stats);
+    if (ctx->stats_host) cudaFreeHost(ctx->stats_host);
     emu_ctx::adjoint_free(ctx);
     emu_ctx_comm_free(ctx);
     if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -632,6 +634,9 @@ int emu_synchronize(emu_context* ctx)
     return EMU_OK;
 }
 
+// loads of at most this many records compute their statistics on the host
+constexpr int64_t kHostStatsMax = 65536;
+
 int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
 {
     if (!ctx || (n > 0 && !records) || n < 0) return fail(ctx, EMU_ERR_ARG, "emu_load_particles: bad arguments");
@@ -639,12 +644,18 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     if ((r = emu_ctx::reserve(ctx, n))) return r;
     CU(cudaMemcpyAsync(ctx->aos, records, sizeof(double) * (size_t)n * ctx->nreal, cudaMemcpyHostToDevice,
                        ctx->stream));
-    // host-side scalars derived from the particles: Vvac_max (Init.cpp:657-660)
-    // and, for the mixed path, the weight sums behind the fixed-point scales
-    double pupt_min = INFINITY;
-    for (int64_t q = 0; q < n; q++) pupt_min = std::min(pupt_min, records[q * ctx->nreal + 3 + 7]);
-    double tot[2] = {0, 0}, mx[2] = {0, 0};
-    if (ctx->mixed) emu_host::weight_totals(ctx->prm, records, n, tot, mx);
+    // scalars derived from the particles: Vvac_max (Init.cpp:657-660) and,
+    // for the mixed path, the weight sums behind the fixed-point scales.  A
+    // small set is scanned on the host while its copy is in flight; a large
+    // one is reduced on the device (one round trip instead of host passes
+    // over the records).
+    double pupt_min = INFINITY, tot[2] = {0, 0}, mx[2] = {0, 0};
+    if (n > kHostStatsMax) {
+        if ((r = emu_ctx::record_stats(ctx, n, pupt_min, tot, mx))) return r;
+    } else {
+        for (int64_t q = 0; q < n; q++) pupt_min = std::min(pupt_min, records[q * ctx->nreal + 3 + 7]);
+        if (ctx->mixed) emu_host::weight_totals(ctx->prm, records, n, tot, mx);
+    }
     return emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx);
 }
 

@@ -55,6 +55,8 @@ struct emu_context {
     void* comm = nullptr;               // ncclComm_t
     int rank = 0, nranks = 1;
     double* red_scratch = nullptr;      // device scalars for load-time reductions
+    double* stats = nullptr;            // per-block record statistics of a load (device)
+    double* stats_host = nullptr;       // and their pinned host copy
     bool adj_valid = false;             // a recorded run matches the slot order
     std::string err;
 };
@@ -85,6 +87,10 @@ int reserve(emu_context* ctx, int64_t n);
 // from this rank's smallest pupt, mixed fixed-point scales from its weight
 // sums and maxima), cell sort, pack, initial deposit
 int load_from_aos(emu_context* ctx, int64_t n, double pupt_min, const double tot[2], const double mx[2]);
+// statistics of the n records in ctx->aos, reduced on the device per block
+// and over the blocks in order on the host (synchronous): smallest pupt,
+// sums and maxima of |N| and |Nbar|
+int record_stats(emu_context* ctx, int64_t n, double& pupt_min, double tot[2], double mx[2]);
 // re-sort the particles by cell now; when perm is not null it receives the
 // gather permutation (new slot i holds old slot perm[i])
 int resort_now(emu_context* ctx, unsigned* perm);

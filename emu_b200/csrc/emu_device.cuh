@@ -271,13 +271,6 @@ __device__ __forceinline__ void atomic_add_mesh(long long* p, long long v)
     atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
 
-// Warp-cooperative deposit.  Every lane of the warp must call it (inactive
-// lanes pass key < 0).  Lanes sharing a stencil (same key) are reduced in
-// registers and one atomic per (cell, component) is issued; with many
-// distinct stencils in a warp each lane adds its own contributions.
-//   val(q, r) returns the contribution of component q (GIdx order minus 3)
-//   before the stencil weight r is applied; conv() turns weight*value into
-//   the accumulation type.
 // ---------------------------------------------------------------------------
 // Tile deposit.  The CTA's particles (consecutive in cell-sorted order) have
 // written one record each to shared memory:

@@ -6,6 +6,8 @@
 // regular load path sorts, packs and deposits.  This file is compiled without
 // FMA contraction, so records agree bit for bit with emu_init_particles
 // except where the record calls sin (simulation type 3) or exp (type 5).
+// The load statistics (smallest pupt, weight sums and maxima) of any record
+// set, the device init's and emu_load_particles', are reduced here too.
 #include "emu_context.cuh"
 #include "emu_init_record.h"
 
@@ -64,6 +66,33 @@ __global__ void __launch_bounds__(kStatBlock) k_record_stats(const double* __res
 
 }  // namespace
 
+constexpr int kStatBlocks = 1184;
+
+int emu_ctx::record_stats(emu_context* ctx, int64_t n, double& pupt_min, double tot[2], double mx[2])
+{
+    if (!ctx->stats) {
+        CU(cudaMalloc(&ctx->stats, sizeof(double) * 5 * kStatBlocks));
+        CU(cudaMallocHost(&ctx->stats_host, sizeof(double) * 5 * kStatBlocks));
+    }
+    const int nblk = (int)std::max<long long>(1, std::min<long long>((n + kStatBlock - 1) / kStatBlock, kStatBlocks));
+    k_record_stats<<<nblk, kStatBlock, 0, ctx->stream>>>(ctx->aos, n, ctx->nreal, ctx->NH, ctx->stats);
+    int r;
+    if ((r = check_launch(ctx, "record statistics"))) return r;
+    CU(cudaMemcpyAsync(ctx->stats_host, ctx->stats, sizeof(double) * 5 * nblk, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const double* hp = ctx->stats_host;
+    pupt_min = INFINITY;
+    tot[0] = tot[1] = mx[0] = mx[1] = 0.0;
+    for (int b = 0; b < nblk; b++) {
+        pupt_min = std::min(pupt_min, hp[5 * b]);
+        tot[0] += hp[5 * b + 1];
+        tot[1] += hp[5 * b + 2];
+        mx[0] = std::max(mx[0], hp[5 * b + 3]);
+        mx[1] = std::max(mx[1], hp[5 * b + 4]);
+    }
+    return EMU_OK;
+}
+
 extern "C" int emu_init_particles_device(emu_context* ctx)
 {
     if (!ctx) return EMU_ERR_ARG;
@@ -77,20 +106,15 @@ extern "C" int emu_init_particles_device(emu_context* ctx)
     int r;
     if ((r = emu_ctx::reserve(ctx, n))) return r;
     double* ddirs = nullptr;
-    double* partial = nullptr;
     int* bad = nullptr;
-    const int nblk = (int)std::min<long long>((n + kStatBlock - 1) / kStatBlock, 1184);
     auto release = [&]() {
         if (ddirs) cudaFree(ddirs);
-        if (partial) cudaFree(partial);
         if (bad) cudaFree(bad);
     };
-    if (cudaMalloc(&ddirs, sizeof(double) * dirs.size()) != cudaSuccess ||
-        cudaMalloc(&partial, sizeof(double) * 5 * nblk) != cudaSuccess || cudaMalloc(&bad, sizeof(int)) != cudaSuccess) {
+    if (cudaMalloc(&ddirs, sizeof(double) * dirs.size()) != cudaSuccess || cudaMalloc(&bad, sizeof(int)) != cudaSuccess) {
         release();
         return fail(ctx, EMU_ERR_NOMEM, "emu_init_particles_device: scratch allocation failed");
     }
-    std::vector<double> hp((size_t)5 * nblk);
     int hbad = 0;
     cudaError_t e = cudaMemcpyAsync(ddirs, dirs.data(), sizeof(double) * dirs.size(), cudaMemcpyHostToDevice,
                                     ctx->stream);
@@ -98,24 +122,15 @@ extern "C" int emu_init_particles_device(emu_context* ctx)
     if (e == cudaSuccess) {
         k_init_records<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(s, ddirs, n, ctx->rank, ctx->nranks,
                                                                                ctx->aos, bad);
-        k_record_stats<<<nblk, kStatBlock, 0, ctx->stream>>>(ctx->aos, n, s.nr, s.nf * s.nf, partial);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(hp.data(), partial, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     release();
     if (e != cudaSuccess)
         return fail(ctx, EMU_ERR_CUDA, std::string("emu_init_particles_device: ") + cudaGetErrorString(e));
     if (hbad) return fail(ctx, EMU_ERR_ARG, "emu_init_particles_device: unknown simulation_type");
-    double pupt_min = INFINITY, tot[2] = {0, 0}, mx[2] = {0, 0};
-    for (int b = 0; b < nblk; b++) {
-        pupt_min = std::min(pupt_min, hp[5 * b]);
-        tot[0] += hp[5 * b + 1];
-        tot[1] += hp[5 * b + 2];
-        mx[0] = std::max(mx[0], hp[5 * b + 3]);
-        mx[1] = std::max(mx[1], hp[5 * b + 4]);
-    }
+    double pupt_min, tot[2], mx[2];
+    if ((r = emu_ctx::record_stats(ctx, n, pupt_min, tot, mx))) return r;
     return emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx);
 }

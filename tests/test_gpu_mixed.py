@@ -106,3 +106,28 @@ def test_mixed_bit_reproducible():
     fc = flavor_cols(3)
     assert colwise_rel(d[inv][:, fc], a[:, fc]) < 1e-5
     assert colwise_rel(d[inv][:, :13], a[:, :13]) < 1e-6
+
+
+@pytest.mark.parametrize("mixed", [True, False])
+def test_large_load_statistics(mixed):
+    """A load of more than 65,536 records reduces its statistics (smallest
+    pupt for Vvac_max, weight sums for the fixed-point scales) on the
+    device: the deposit and compute_dt agree with the oracle as for small
+    loads"""
+    p = W.c3_three_flavor_1d(ncell_z=256, mixed=mixed)
+    p.precision = api.PREC_MIXED if mixed else api.PREC_FP64
+    parts = api.init_particles(p)
+    assert parts.shape[0] > 65536
+    o = Oracle(p)
+    ref = o.deposit(parts)
+    with api.Context(p) as c:
+        c.load_particles(parts)
+        mesh = c.get_mesh()
+        dt, _ = c.compute_dt()
+    dto, _ = o.compute_dt(ref, o.vvac_max(parts))
+    if mixed:
+        assert mesh_rel_mag(mesh, ref, magnitude_mesh(o, parts), 3 + 72) < 1e-6
+        assert abs(dt - dto) <= 1e-6 * dto
+    else:
+        assert mesh_rel_mag(mesh, ref, magnitude_mesh(o, parts), 3 + 72) < 1e-12
+        assert abs(dt - dto) <= 1e-12 * dto
