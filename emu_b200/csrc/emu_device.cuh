@@ -367,10 +367,79 @@ struct RunAcc<float, S, SP> {
 // of equal stencil keys in registers and adds the run total with one atomic
 // per (cell, component).  Inside a run, aligned groups of four records with
 // the run's key are summed without per-record key tests.
+// FP32, three flavors, 27-cell stencils: a thread owns the component pair
+// (q, q + 36) (same f N, velocity factors d and d + 2), so that one load of a
+// record's 27 weights and f N serves 54 run sums; 36 pairs per stream, three
+// streams of records per 128-thread CTA (a component per thread leaves one
+// stream of 72 threads).
+template <int BLOCK, int NTILE, class SWt, class T, class Conv>
+__device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, const int* skey, const float* srec,
+                                                   int ntile, Conv conv)
+{
+    using TR = TileRec<3, SWt, float>;
+    constexpr int NH = 9, NS = 18, ND = 72, NQ = ND / 2, RW = TR::RW, SP = TR::SP, S = TR::S;
+    constexpr int NSTREAM = BLOCK / NQ;
+    constexpr int CH = (NTILE + NSTREAM - 1) / NSTREAM;
+    const int q0 = threadIdx.x % NQ;
+    const int stream = threadIdx.x / NQ;
+    if (stream >= NSTREAM) return;   // no block-wide barrier follows inside
+    const int q1 = q0 + NQ;
+    const int dir0 = q0 / (2 * NH), sp = (q0 / NH) & 1, e = q0 % NH;   // dir1 = dir0 + 2
+    const int boff = SP + sp * NH + e;
+    const int voff0 = SP + NS + (dir0 > 0 ? dir0 - 1 : 0);
+    const int voff1 = SP + NS + dir0 + 1;
+    RunAcc<float, S, SP> acc0, acc1;
+    auto flush = [&](int key) {
+        const int bx = key % P.n[0];
+        const int by = (key / P.n[0]) % P.n[1];
+        const int bz = key / (P.n[0] * P.n[1]);
+#pragma unroll
+        for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+            for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+                for (int ii = 0; ii < SWt::MX; ii++) {
+                    if (!SWt::on(P, ii, jj, kk)) continue;
+                    const int k = (kk * SWt::MY + jj) * SWt::MX + ii;
+                    T* m = &mesh[cell_of(P, bx, by, bz, ii, jj, kk) * ND];
+                    const T v0 = conv(acc0.get(k), sp), v1 = conv(acc1.get(k), sp);
+                    if (v0 != (T)0) atomic_add_mesh(m + q0, v0);
+                    if (v1 != (T)0) atomic_add_mesh(m + q1, v1);
+                }
+    };
+    const int i1 = min((stream + 1) * CH, ntile);
+    int cur = -1;
+    acc0.zero();
+    acc1.zero();
+    for (int i = stream * CH; i < i1; i++) {
+        const int key = skey[i];
+        if (key != cur) {
+            if (cur >= 0) flush(cur);
+            acc0.zero();
+            acc1.zero();
+            cur = key;
+        }
+        if (key < 0) continue;
+        const float* r = srec + i * RW;
+        const float b = r[boff];
+        const float qv0 = dir0 == 0 ? b : b * r[voff0];
+        const float qv1 = b * r[voff1];
+        float w[SP];
+        load_weights<float, SP>(r, w);
+        acc0.add(w, qv0);
+        acc1.add(w, qv1);
+    }
+    if (cur >= 0) flush(cur);
+}
+
 template <int NF, int BLOCK, int NTILE, class SWt, class R, class T, class Conv>
 __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const R* srec, int ntile,
                                              Conv conv)
 {
+    if constexpr (NF == 3 && sizeof(R) == 4 && SWt::MX * SWt::MY * SWt::MZ == 27 && BLOCK >= 72) {
+        tile_deposit_pairs<BLOCK, NTILE, SWt, T>(P, mesh, skey, reinterpret_cast<const float*>(srec), ntile, conv);
+        return;
+    }
     using TR = TileRec<NF, SWt, R>;
     constexpr int NH = NF * NF, NS = 2 * NH, ND = 8 * NH, RW = TR::RW, SP = TR::SP;
     constexpr int NDP = (ND + 31) / 32 * 32;
