@@ -163,7 +163,9 @@ int ensure_capacity(emu_context* ctx, long long n)
     ctx->keys = ctx->keys2 = ctx->idx = ctx->idx2 = nullptr;
     ctx->sort_tmp = nullptr;
     ctx->S[0].kgen = ctx->S[1].kgen = nullptr;
-    const long long cap = std::max<long long>(n, 1);
+    // whole 128-particle tiles: every CTA's slice of a state array is a
+    // 16-byte aligned block that bulk copies may read in full
+    const long long cap = (std::max<long long>(n, 1) + 127) / 128 * 128;
     for (int i = 0; i < 2; i++) {
         CU(cudaMalloc(&ctx->pblock[i], persistent_bytes(ctx->NS, ctx->mixed, cap)));
         ctx->S[i] = DevState();

@@ -156,6 +156,46 @@ __device__ __forceinline__ void zero_slice(T* buf, long long n)
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Bulk copies global -> shared on the TMA engine (cp.async.bulk, no
+// multicast) completing on an mbarrier: a CTA stages its particles' state
+// arrays (one contiguous 128-particle slice per component) while its threads
+// do other work.  Addresses and sizes are multiples of 16 bytes (particle
+// capacities are multiples of 128).
+__device__ __forceinline__ unsigned smem_u32(const void* ptr) { return (unsigned)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// wait for phase `parity` of the barrier, at most kMbarPolls polls (each
+// try_wait may suspend the thread for a while); false when it gave up
+constexpr int kMbarPolls = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    const unsigned a = smem_u32(bar);
+    for (int i = 0; i < kMbarPolls; i++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // ===========================================================================
 // compute_dt pieces (Evolve.cpp:57-124 + compute_dt fill)
 // ===========================================================================
@@ -1127,6 +1167,18 @@ __device__ __forceinline__ void potential_si32(const DevParams& P, const float* 
     })
 }
 
+// dynamic shared memory of a mixed stage: the deposit tile, or the staged
+// state slices (f0 FP64, k32 and ksum32 FP32) when those are larger
+template <int NF, int WX, int WY, int WZ>
+constexpr int mixed_stage_smem_bytes()
+{
+    constexpr int tile = tile_smem_bytes<NF, SW<WX, WY, WZ>, float>();
+    using SWt = SW<WX, WY, WZ>;
+    constexpr bool preload = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
+    constexpr int staged = preload ? 0 : 2 * NF * NF * kBlock * 16;
+    return tile > staged ? tile : staged;
+}
+
 template <int NF, int WX, int WY, int WZ>
 // (1D: 5 CTAs per SM at 96 registers beat 4 at 128 despite the spills)
 __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S, int s,
@@ -1139,6 +1191,10 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
     constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
+    // without the register preload, the CTA's slices of f0, k32 and ksum32
+    // are staged in shared memory by bulk copies (the record area of the
+    // deposit, written only after the state is consumed)
+    constexpr bool STAGE = !PRELOAD;
     // (programmatic dependent launch: see grid_dep_wait; the finalize
     // kernel before this stage has waited for the previous stage)
     const int done = __ldcg(&ctl->done);
@@ -1147,6 +1203,26 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
     const long long cap = S.cap;
+    const int t = threadIdx.x;
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    __shared__ __align__(8) unsigned long long stage_bar;
+    double* const sf0 = reinterpret_cast<double*>(tile_smem);        // [NS][kBlock]
+    float* const sk = reinterpret_cast<float*>(sf0 + NS * kBlock);   // [NS][kBlock]
+    float* const sks = sk + NS * kBlock;                             // [NS][kBlock]
+    const long long p0 = (long long)blockIdx.x * kBlock;
+    if constexpr (STAGE) {
+        // f0 is written only by the previous step: its copies start before
+        // the dependency wait, k32 and ksum32 (the previous stage's) after it
+        if (t < 32) {
+            if (t == 0) {
+                mbar_init(&stage_bar, 1);
+                mbar_expect_tx(&stage_bar, NS * kBlock * 8 + (s > 1 ? 2 * NS * kBlock * 4 : 0));
+            }
+            __syncwarp();
+            for (int c = t; c < NS; c += 32) bulk_g2s(sf0 + c * kBlock, S.f0 + c * cap + p0, kBlock * 8, &stage_bar);
+        }
+        __syncthreads();   // the barrier is initialised before anyone waits on it
+    }
 
     // prologue: fields that no kernel of this step writes (one memory round
     // trip with the control loads; all of the state at the step start for
@@ -1186,6 +1262,13 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     }
     grid_dep_wait();
     grid_dep_launch();
+    if constexpr (STAGE) {
+        if (s > 1 && t < 32)
+            for (int c = t; c < 2 * NS; c += 32) {
+                const float* src = c < NS ? S.k32 + c * cap + p0 : S.ksum32 + (c - NS) * cap + p0;
+                bulk_g2s(sk + c * kBlock, src, kBlock * 4, &stage_bar);
+            }
+    }
     // compute_dt on the stage-4 mesh (every block has read this step's dt)
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
     if (active) {
@@ -1216,20 +1299,22 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         const double an = s < 4 ? dt * kRK4A[s] : 0.0;
         const double w6 = dt * (1.0 / 6.0);
         int stt = 0;
+        if constexpr (STAGE) {
+            if (!mbar_wait(&stage_bar, 0)) atomicOr(&ctl->status, ST_TIMEOUT);
+        }
         // one species at a time keeps the live state small
 #pragma unroll
         for (int sp = 0; sp < 2; sp++) {
             double y0[NH], f[NH];
 #pragma unroll
             for (int e = 0; e < NH; e++) {
-                const long long o = (sp * NH + e) * cap + p;
                 float k;
                 if constexpr (PRELOAD) {
                     y0[e] = y0a[sp * NH + e];
                     k = ka[sp * NH + e];
                 } else {
-                    y0[e] = f0p[o];
-                    k = s > 1 ? k32p[o] : 0.f;
+                    y0[e] = sf0[(sp * NH + e) * kBlock + t];
+                    k = s > 1 ? sk[(sp * NH + e) * kBlock + t] : 0.f;
                 }
                 f[e] = s > 1 ? y0[e] + aw * (double)k : y0[e];
             }
@@ -1255,7 +1340,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     const float kc = (float)(Kv[e] + (double)ksi[e]);
                     float ks;
                     if constexpr (PRELOAD) ks = ksa[sp * NH + e];
-                    else ks = s > 1 ? ks32p[o] : 0.f;
+                    else ks = s > 1 ? sks[(sp * NH + e) * kBlock + t] : 0.f;
                     S.k32[o] = kc;
                     S.ksum32[o] = (s == 1) ? kc : fmaf(2.f, kc, ks);
                     fn[e] = y0[e] + an * (double)kc;
@@ -1263,10 +1348,9 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
             } else {
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
-                    const long long o = (sp * NH + e) * cap + p;
                     float ks;
                     if constexpr (PRELOAD) ks = ksa[sp * NH + e];
-                    else ks = ks32p[o];
+                    else ks = sks[(sp * NH + e) * kBlock + t];
                     fn[e] = y0[e] + w6 * ((double)ks + (Kv[e] + (double)ksi[e]));
                 }
                 stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : S.Ll[sp][p], P.maxError);
@@ -1300,6 +1384,12 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
             report_bad(ctl, stt, S.id[p]);
             make_stencil<float>(P, xn[0], xn[1], xn[2], st);
         }
+    }
+    if constexpr (STAGE) {
+        // the staged state is consumed (and the copies complete) before the
+        // deposit records reuse the area
+        if (t == 0 && !mbar_wait(&stage_bar, 0)) atomicOr(&ctl->status, ST_TIMEOUT);
+        __syncthreads();
     }
     if (qout)
         tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4 || P.rank_stages);
@@ -1699,8 +1789,8 @@ void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, cons
                               const long long* qdt, StepCtl* ctl, int dt_mode, cudaStream_t st)
 {
     EMU_W_DISPATCH(P, (launch_pdl(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock,
-                                  tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>(), st, P, S, s, gmesh, qout, qdt,
-                                  ctl, dt_mode)));
+                                  mixed_stage_smem_bytes<NF, WXv, WYv, WZv>(), st, P, S, s, gmesh, qout, qdt, ctl,
+                                  dt_mode)));
 }
 
 template <int NF>
