@@ -367,9 +367,9 @@ struct RunAcc<float, S, SP> {
 // of equal stencil keys in registers and adds the run total with one atomic
 // per (cell, component).  Inside a run, aligned groups of four records with
 // the run's key are summed without per-record key tests.
-// FP32, three flavors, 27-cell stencils: a thread owns the component pair
-// (q, q + 36) (same f N, velocity factors d and d + 2), so that one load of a
-// record's 27 weights and f N serves 54 run sums; 36 pairs per stream, three
+// FP32, three flavors: a thread owns the component pair (q, q + 36) (same
+// f N, velocity factors d and d + 2), so that one load of a record's stencil
+// weights and f N serves two run sums per cell; 36 pairs per stream, three
 // streams of records per 128-thread CTA (a component per thread leaves one
 // stream of 72 threads).
 template <int BLOCK, int NTILE, class SWt, class T, class Conv>
@@ -436,7 +436,7 @@ template <int NF, int BLOCK, int NTILE, class SWt, class R, class T, class Conv>
 __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const R* srec, int ntile,
                                              Conv conv)
 {
-    if constexpr (NF == 3 && sizeof(R) == 4 && SWt::MX * SWt::MY * SWt::MZ == 27 && BLOCK >= 72) {
+    if constexpr (NF == 3 && sizeof(R) == 4 && BLOCK >= 72) {
         tile_deposit_pairs<BLOCK, NTILE, SWt, T>(P, mesh, skey, reinterpret_cast<const float*>(srec), ntile, conv);
         return;
     }
