@@ -245,20 +245,40 @@ int zero_mesh(emu_context* ctx, int i)
     return EMU_OK;
 }
 
+// mixed path: full deposit of the current state into qfull (summed over the
+// ranks)
+int deposit_full_q(emu_context* ctx)
+{
+    const DevState& S = ctx->S[ctx->cur];
+    CU(cudaMemsetAsync(ctx->qfull, 0, sizeof(long long) * mesh_elems(ctx), ctx->stream));
+    emu::launch_deposit_q(ctx->nf, ctx->P, S, S.f0, ctx->qfull, ctx->stream);
+    int r;
+    if ((r = check_launch(ctx, "full deposit"))) return r;
+    return emu_ctx::reduce_mesh(ctx, ctx->qfull, true, ctx->stream);
+}
+
+// the full mesh of the mixed path that the API reads: the last deposit's
+// (after a load or emu_deposit) or the stage-4 mesh M_4 (after steps)
+long long* q_current(emu_context* ctx) { return ctx->cur_mesh == 0 ? ctx->qfull : ctx->qmesh[1]; }
+
 // deposit of the current state into mesh slot 0 and a clean slot 1: the
-// state the fused step loop expects at a step boundary
+// state the fused step loop expects at a step boundary (mixed path: the full
+// deposit in qfull, converted into the combined layout of slot 0)
 int deposit_current(emu_context* ctx)
 {
-    DevState& S = ctx->S[ctx->cur];
+    const DevState& S = ctx->S[ctx->cur];
     int r;
     if ((r = zero_mesh(ctx, 0))) return r;
     if ((r = zero_mesh(ctx, 1))) return r;
-    if (ctx->mixed) emu::launch_deposit_q(ctx->nf, ctx->P, S, S.f0, ctx->qmesh[0], ctx->stream);
-    else emu::launch_deposit(ctx->nf, ctx->P, S, S.f0, ctx->mesh[0], ctx->stream);
-    if ((r = check_launch(ctx, "deposit"))) return r;
-    if (ctx->mixed) r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[0], true, ctx->stream);
-    else r = emu_ctx::reduce_mesh(ctx, ctx->mesh[0], false, ctx->stream);
-    if (r) return r;
+    if (ctx->mixed) {
+        if ((r = deposit_full_q(ctx))) return r;
+        emu::launch_full_to_comb(ctx->nf, ctx->P, ctx->qfull, ctx->qmesh[0], ctx->stream);
+        if ((r = check_launch(ctx, "combined mesh"))) return r;
+    } else {
+        emu::launch_deposit(ctx->nf, ctx->P, S, S.f0, ctx->mesh[0], ctx->stream);
+        if ((r = check_launch(ctx, "deposit"))) return r;
+        if ((r = emu_ctx::reduce_mesh(ctx, ctx->mesh[0], false, ctx->stream))) return r;
+    }
     ctx->cur_mesh = 0;
     ctx->fused_ready = true;
     return EMU_OK;
@@ -288,7 +308,8 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt, bool dep4
     int a = 0;
     for (int s = 1; s <= 4; s++) {
         const int b = 1 - a;
-        emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, st);
+        // M_1..M_3 in the combined layout, M_4 full
+        emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, s != 4, st);
         // M_4 sits in q[1] (read by stage 4's compute_dt) until the next
         // step's first finalize zeroes it
         const bool dep = s < 4 || dep4;
@@ -481,6 +502,12 @@ int emu_ctx::load_from_aos(emu_context* ctx, int64_t n, double pupt_min, const d
         if ((r = emu_ctx_reduce_scalars(ctx, mx, 2, 1))) return r;
         if (!emu_host::fixed_point_scales_from(tot, mx, ctx->P.q_scale, ctx->P.q_unscale, why))
             return fail(ctx, EMU_ERR_LIMIT, "load: " + why);
+        // the combined self-interaction mesh sums both species
+        double tg[2] = {tot[0] + tot[1], tot[0] + tot[1]}, mg[2], gs[2], gu[2];
+        mg[0] = mg[1] = std::max(mx[0], mx[1]);
+        if (!emu_host::fixed_point_scales_from(tg, mg, gs, gu, why)) return fail(ctx, EMU_ERR_LIMIT, "load: " + why);
+        ctx->P.g_scale = gs[0];
+        ctx->P.g_unscale = gu[0];
     }
     emu::launch_cell_keys(ctx->P, ctx->aos, ctx->nreal, n, ctx->keys, ctx->idx, ctx->stream);
     if ((r = sort_perm(ctx, n))) return r;
@@ -566,6 +593,7 @@ int emu_create(const emu_params* p, emu_context** out)
     if (ctx->mixed) {
         for (int i = 0; i < 2 && !r; i++)
             if (cudaMalloc(&ctx->qmesh[i], sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+        if (!r && cudaMalloc(&ctx->qfull, sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
         if (!r && cudaMalloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * 4 * ctx->NH) != cudaSuccess)
             r = EMU_ERR_NOMEM;
     } else {
@@ -586,6 +614,7 @@ int emu_create(const emu_params* p, emu_context** out)
         if (ctx->mesh[i]) cudaMemset(ctx->mesh[i], 0, sizeof(double) * me);
     for (int i = 0; i < 2; i++)
         if (ctx->qmesh[i]) cudaMemset(ctx->qmesh[i], 0, sizeof(long long) * me);
+    if (ctx->qfull) cudaMemset(ctx->qfull, 0, sizeof(long long) * me);
     if (cudaDeviceSynchronize() != cudaSuccess) {
         ctx->err = "emu_create: device initialisation failed";
         return bail(EMU_ERR_CUDA);
@@ -604,6 +633,7 @@ void emu_destroy(emu_context* ctx)
     if (ctx->S[0].kgen) cudaFree(ctx->S[0].kgen);
     for (int i = 0; i < 4; i++) if (ctx->mesh[i]) cudaFree(ctx->mesh[i]);
     for (int i = 0; i < 2; i++) if (ctx->qmesh[i]) cudaFree(ctx->qmesh[i]);
+    if (ctx->qfull) cudaFree(ctx->qfull);
     if (ctx->gmesh) cudaFree(ctx->gmesh);
     if (ctx->fmesh_tmp) cudaFree(ctx->fmesh_tmp);
     if (ctx->planes) cudaFree(ctx->planes);
@@ -698,7 +728,7 @@ int emu_get_mesh(emu_context* ctx, double* out)
 {
     if (!ctx || !out) return fail(ctx, EMU_ERR_ARG, "emu_get_mesh: bad arguments");
     const long long nc = ctx->P.ncells;
-    if (ctx->mixed) emu::launch_mesh_out_q(ctx->nf, ctx->P, ctx->qmesh[ctx->cur_mesh], ctx->planes, ctx->stream);
+    if (ctx->mixed) emu::launch_mesh_out_q(ctx->nf, ctx->P, q_current(ctx), ctx->planes, ctx->stream);
     else emu::launch_mesh_out(ctx->nf, ctx->P, ctx->mesh[ctx->cur_mesh], ctx->planes, ctx->stream);
     int r;
     if ((r = check_launch(ctx, "mesh out"))) return r;
@@ -727,7 +757,7 @@ int emu_interpolate_rhs(emu_context* ctx, double* rhs_records)
     if (ctx->mixed) {
         // the FP64 interpolation of the fixed-point mesh
         if (!ctx->fmesh_tmp) CU(cudaMalloc(&ctx->fmesh_tmp, sizeof(double) * mesh_elems(ctx)));
-        emu::launch_q_to_f64(ctx->nf, ctx->P, ctx->qmesh[ctx->cur_mesh], ctx->fmesh_tmp, ctx->stream);
+        emu::launch_q_to_f64(ctx->nf, ctx->P, q_current(ctx), ctx->fmesh_tmp, ctx->stream);
         mesh = ctx->fmesh_tmp;
     } else {
         mesh = ctx->mesh[ctx->cur_mesh];
@@ -760,7 +790,7 @@ int emu_compute_dt(emu_context* ctx, double* dt)
 {
     if (!ctx || !dt) return EMU_ERR_ARG;
     emu::launch_ctl_set(ctx->ctl, 0.0, 0.0, 0.0, 1, 1, ctx->stream);
-    if (ctx->mixed) emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[ctx->cur_mesh], ctx->ctl, emu::DT_QUERY, ctx->stream);
+    if (ctx->mixed) emu::launch_dt_q(ctx->nf, ctx->P, q_current(ctx), ctx->ctl, emu::DT_QUERY, ctx->stream);
     else emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[ctx->cur_mesh], ctx->ctl, emu::DT_QUERY, ctx->stream);
     int r;
     if ((r = check_launch(ctx, "compute_dt"))) return r;
@@ -808,7 +838,12 @@ int emu_evolve_begin(emu_context* ctx, double start_time, double end_time, int m
     int r;
     if (!ctx->fused_ready && (r = deposit_current(ctx))) return r;
     emu::launch_ctl_set(ctx->ctl, 0.0, start_time, end_time, max_steps, 1, ctx->stream);
-    if (ctx->mixed) emu::launch_dt_q(ctx->nf, ctx->P, ctx->qmesh[0], ctx->ctl, emu::DT_INIT, ctx->stream);
+    if (ctx->mixed) {
+        // the full mesh of the current state (after steps the step's first
+        // mesh holds only the combined layout)
+        if (ctx->cur_mesh != 0 && (r = deposit_full_q(ctx))) return r;
+        emu::launch_dt_q(ctx->nf, ctx->P, ctx->qfull, ctx->ctl, emu::DT_INIT, ctx->stream);
+    }
     else emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[0], ctx->ctl, emu::DT_INIT, ctx->stream);
     return check_launch(ctx, "initial compute_dt");
 }
@@ -905,7 +940,8 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
         for (int s = 1; s <= 4; s++) {
             const int b = 1 - a;
             rec(2 * k);
-            emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, st);
+            emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, s != 4,
+                                       st);
             rec(2 * k + 1);
             k++;
             rec(2 * k);

@@ -29,6 +29,10 @@ struct emu_context {
     long long cap = 0;
     double* mesh[4] = {nullptr, nullptr, nullptr, nullptr};
     long long* qmesh[2] = {nullptr, nullptr};
+    // mixed path: the full 8 NF^2 mesh of the state at the last deposit
+    // (the step meshes M_1..M_3 hold only the combined self-interaction
+    // layout; M_4 and this one are full, for compute_dt and the outputs)
+    long long* qfull = nullptr;
     float* gmesh = nullptr;
     double* fmesh_tmp = nullptr;        // FP64 cell-major copy (mixed API calls)
     double* planes = nullptr;           // ncomp x ncells output staging

@@ -60,6 +60,7 @@ struct DevParams {
     long long ncells;
     int key_bits;      // bits of a stencil key in [0, ncells]
     int rank_stages;   // particles may have moved since the last re-sort: every deposit ranks its keys
+    double g_scale, g_unscale;   // fixed point of the mixed path's self-interaction mesh (both species)
     double L[3];       // domain length (periodic, [0,L))
     double dxi[3];     // inverse cell size
     double sqrt2GF_inv_vol;   // sqrt(2)*GF*inv_cell_volume (Evolve.cpp:167 + fill)
@@ -432,6 +433,64 @@ __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, 
     if (cur >= 0) flush(cur);
 }
 
+// Combined deposit of the mixed path (FP32 records): per cell the 4 NF^2
+// self-interaction combinations G[d][e] = sum w v_d (fN_nu,e - s_e fN_nubar,e)
+// (v_0 = 1; s_e = -1 for imaginary components: the sign rule of the
+// potential), which is all a stage's interpolation reads.  Records hold the
+// NF^2 combinations c_e; thread q = (d, e) of NSTREAM = BLOCK / (4 NF^2)
+// record streams sums its runs and adds them to mesh[cell * 4 NF^2 + q].
+template <int NF, int BLOCK, int NTILE, class SWt, class T, class Conv>
+__device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, const int* skey, const float* srec,
+                                                  int ntile, Conv conv)
+{
+    using TR = TileRec<NF, SWt, float>;
+    constexpr int NH = NF * NF, NS = 2 * NH, NG = 4 * NH, RW = TR::RW, SP = TR::SP, S = TR::S;
+    constexpr int NSTREAM = BLOCK / NG;
+    static_assert(NSTREAM >= 1, "one stream of components");
+    constexpr int CH = (NTILE + NSTREAM - 1) / NSTREAM;
+    const int q = threadIdx.x % NG;
+    const int stream = threadIdx.x / NG;
+    if (stream >= NSTREAM) return;   // no block-wide barrier follows inside
+    const int d = q / NH, e = q % NH;
+    const int coff = SP + e;
+    const int voff = SP + NS + (d > 0 ? d - 1 : 0);
+    RunAcc<float, S, SP> acc;
+    auto flush = [&](int key) {
+        const int bx = key % P.n[0];
+        const int by = (key / P.n[0]) % P.n[1];
+        const int bz = key / (P.n[0] * P.n[1]);
+#pragma unroll
+        for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+            for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+                for (int ii = 0; ii < SWt::MX; ii++) {
+                    if (!SWt::on(P, ii, jj, kk)) continue;
+                    const T v = conv(acc.get((kk * SWt::MY + jj) * SWt::MX + ii), 0);
+                    if (v != (T)0) atomic_add_mesh(&mesh[cell_of(P, bx, by, bz, ii, jj, kk) * NG + q], v);
+                }
+    };
+    const int i1 = min((stream + 1) * CH, ntile);
+    int cur = -1;
+    acc.zero();
+    for (int i = stream * CH; i < i1; i++) {
+        const int key = skey[i];
+        if (key != cur) {
+            if (cur >= 0) flush(cur);
+            acc.zero();
+            cur = key;
+        }
+        if (key < 0) continue;
+        const float* r = srec + i * RW;
+        const float b = r[coff];
+        const float qv = d == 0 ? b : b * r[voff];
+        float w[SP];
+        load_weights<float, SP>(r, w);
+        acc.add(w, qv);
+    }
+    if (cur >= 0) flush(cur);
+}
+
 template <int NF, int BLOCK, int NTILE, class SWt, class R, class T, class Conv>
 __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const int* skey, const R* srec, int ntile,
                                              Conv conv)
@@ -508,12 +567,15 @@ __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const 
 }
 
 // write one particle's deposit record (phase A of the tile deposit)
-template <int NF, class SWt, class R>
+// (NV values per particle: f N of both species, or the NF^2 self-interaction
+// combinations of the combined deposit; v always sits after 2 NF^2 slots)
+template <int NF, class SWt, class R, int NV = 2 * NF * NF>
 __device__ __forceinline__ void tile_record(R* srec, int* skey, int i, int key, const R* fN, R vx, R vy, R vz,
                                             const Stencil<R>& st)
 {
     using TR = TileRec<NF, SWt, R>;
     constexpr int NS = TR::NS, RW = TR::RW, SP = TR::SP;
+    static_assert(NV <= NS, "record values");
     skey[i] = key;
     R* r = srec + i * RW;
 #pragma unroll
@@ -526,7 +588,7 @@ __device__ __forceinline__ void tile_record(R* srec, int* skey, int i, int key, 
 #pragma unroll
     for (int k = TR::S; k < SP; k++) r[k] = (R)0;
 #pragma unroll
-    for (int c = 0; c < NS; c++) r[SP + c] = fN[c];
+    for (int c = 0; c < NV; c++) r[SP + c] = fN[c];
     r[SP + NS + 0] = vx;
     r[SP + NS + 1] = vy;
     r[SP + NS + 2] = vz;

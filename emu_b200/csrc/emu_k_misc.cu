@@ -145,15 +145,21 @@ static unsigned reduce_grid(long long ncells)
 }
 
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
-                           StepCtl* ctl, cudaStream_t st)
+                           StepCtl* ctl, bool comb, cudaStream_t st)
 {
     EMU_NF_DISPATCH(nf, (launch_pdl(k_finalize_mixed<NFv>, reduce_grid(P.ncells * 4 * NFv * NFv), kBlock, 0, st, P,
-                                    qread, qzero, gmesh, ctl)));
+                                    qread, qzero, gmesh, ctl, comb ? 1 : 0)));
 }
 
 void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st)
 {
     EMU_NF_DISPATCH(nf, (k_dt<NFv, double><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode)));
+}
+
+void launch_full_to_comb(int nf, const DevParams& P, const long long* qfull, long long* qcomb, cudaStream_t st)
+{
+    EMU_NF_DISPATCH(nf, (k_full_to_comb<NFv><<<reduce_grid(P.ncells * 4 * NFv * NFv), kBlock, 0, st>>>(P, qfull,
+                                                                                                        qcomb)));
 }
 
 void launch_dt_q(int nf, const DevParams& P, const long long* mesh, StepCtl* ctl, int mode, cudaStream_t st)

@@ -94,9 +94,12 @@ cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, 
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
                             long long* qmesh_out, const long long* qmesh_dt, StepCtl* ctl, int dt_mode,
                             cudaStream_t st);
+// comb: qread holds the combined layout (else the full mesh)
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
-                           StepCtl* ctl, cudaStream_t st);
+                           StepCtl* ctl, bool comb, cudaStream_t st);
 void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st);
+// a full int64 mesh in the combined layout (mixed path)
+void launch_full_to_comb(int nf, const DevParams& P, const long long* qfull, long long* qcomb, cudaStream_t st);
 void launch_dt_q(int nf, const DevParams& P, const long long* mesh, StepCtl* ctl, int mode, cudaStream_t st);
 void launch_renorm(int nf, const DevParams& P, const DevState& S, StepCtl* ctl, cudaStream_t st);
 void launch_mesh_out(int nf, const DevParams& P, const double* mesh, double* out, cudaStream_t st);

@@ -382,6 +382,20 @@ struct QuantConv {
         return __float2ll_rn(a * (float)P.q_scale[sp]);
     }
 };
+// (the combined self-interaction mesh: one scale for both species)
+struct QuantConvG {
+    const DevParams& P;
+    __device__ long long operator()(float a, int) const { return __float2ll_rn(a * (float)P.g_scale); }
+};
+// the NF^2 self-interaction combinations of a particle's f N (nu minus nubar,
+// nu plus nubar for imaginary components: the potential's sign rule)
+template <int NF>
+__device__ __forceinline__ void combine_species(const float* fN, float* c)
+{
+    constexpr int NH = NF * NF;
+#pragma unroll
+    for (int e = 0; e < NH; e++) c[e] = Herm<NF>::is_im(e) ? fN[e] + fN[NH + e] : fN[e] - fN[NH + e];
+}
 
 // Stable rank of the stencil keys held by the first NW warps of the block
 // (key -1 = inactive, ranked last): the permutation a stable sort of the
@@ -484,7 +498,8 @@ __device__ __forceinline__ bool distinct_key_rank(int key, int* scratch, int& sl
 // that moved since the last re-sort; the deposit of moved particles at the
 // end of a step): the 128 keys are ranked first (stable, so cell-sorted
 // particles keep their order), so that each stencil forms one run
-template <int NF, class SWt, class R, class T, class Conv>
+// COMB: the mixed path's combined deposit (fN holds the NF^2 combinations)
+template <int NF, class SWt, class R, class T, class Conv, bool COMB = false>
 __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
                                                    const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false)
 {
@@ -514,9 +529,15 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
             slot = srank[threadIdx.x];
         }
     }
-    tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
-    __syncthreads();
-    tile_deposit<NF, kBlock, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
+    if constexpr (COMB) {
+        tile_record<NF, SWt, R, NF * NF>(srec, skey, slot, key, fN, vx, vy, vz, st);
+        __syncthreads();
+        tile_deposit_comb<NF, kBlock, kBlock, SWt, T>(P, mesh, skey, srec, kBlock, conv);
+    } else {
+        tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
+        __syncthreads();
+        tile_deposit<NF, kBlock, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
+    }
 }
 
 // The same for a species-split CTA (kBlock particles, 2 kBlock threads:
@@ -1091,7 +1112,7 @@ __global__ void __launch_bounds__(kBlock) k_dt(DevParams P, const T* __restrict_
 template <int NF>
 __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const long long* __restrict__ q,
                                                            long long* __restrict__ qzero, float* __restrict__ g,
-                                                           StepCtl* ctl)
+                                                           StepCtl* ctl, int comb)
 {
     using H = Herm<NF>;
     constexpr int NH = NF * NF, ND = 8 * NH, NG = 4 * NH;
@@ -1101,6 +1122,13 @@ __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const lo
     zero_slice(qzero, qzero ? P.ncells * ND : 0);
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long total = P.ncells * NG;
+    if (comb) {
+        // a combined mesh holds G itself
+        const double f = P.sqrt2GF_inv_vol * P.g_unscale;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+            g[i] = (float)((double)q[i] * f);
+        return;
+    }
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         const long long c = i / NG;
         const int k = (int)(i - c * NG);
@@ -1110,6 +1138,27 @@ __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const lo
         const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
         const double comb = H::is_im(e) ? a + b : a - b;
         g[i] = (float)(P.sqrt2GF_inv_vol * comb);
+    }
+}
+
+// full int64 mesh (8 NF^2 per cell, a scale per species) -> the combined
+// self-interaction layout of the step meshes (4 NF^2 per cell, one scale)
+template <int NF>
+__global__ void __launch_bounds__(kBlock) k_full_to_comb(DevParams P, const long long* __restrict__ q,
+                                                         long long* __restrict__ out)
+{
+    using H = Herm<NF>;
+    constexpr int NH = NF * NF, ND = 8 * NH, NG = 4 * NH;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long total = P.ncells * NG;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long c = i / NG;
+        const int k = (int)(i - c * NG);
+        const int d = k / NH, e = k - d * NH;
+        const long long* m = q + c * ND;
+        const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
+        const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
+        out[i] = __double2ll_rn((H::is_im(e) ? a + b : a - b) * P.g_scale);
     }
 }
 
@@ -1391,8 +1440,20 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         if (t == 0 && !mbar_wait(&stage_bar, 0)) atomicOr(&ctl->status, ST_TIMEOUT);
         __syncthreads();
     }
-    if (qout)
-        tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, s == 4 || P.rank_stages);
+    if (qout) {
+        if (s == 3) {
+            // M_4, the mesh compute_dt reads (N, Nbar and the fluxes apart):
+            // the full layout
+            tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, P.rank_stages != 0);
+        } else {
+            // M_2, M_3 and the next step's M_1: only the combinations the
+            // stages interpolate
+            float cN[NH];
+            combine_species<NF>(fN, cN);
+            tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(P, qout, active, st, cN, vx, vy, vz,
+                                                                            QuantConvG{P}, s == 4 || P.rank_stages);
+        }
+    }
 }
 
 // ===========================================================================
@@ -1562,8 +1623,13 @@ __global__ void __launch_bounds__(kBlock) k_gather_deposit(DevParams P, DevState
         }
         make_stencil<R>(P, x[0], x[1], x[2], st);
     }
-    if constexpr (MIXED) tile_deposit_block<NF, SWt, float>(P, qmesh, active, st, fN, vx, vy, vz, QuantConv{P});
-    else
+    if constexpr (MIXED) {
+        // the next step's first mesh: the combined layout
+        float cN[NH];
+        combine_species<NF>(fN, cN);
+        tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(P, qmesh, active, st, cN, vx, vy, vz,
+                                                                        QuantConvG{P});
+    } else
         tile_deposit_block<NF, SWt, double>(P, mesh, active, st, fN, vx, vy, vz,
                                             [](double a, int) -> double { return a; });
 }
