@@ -102,8 +102,8 @@ size_t persistent_bytes(int NS, bool mixed, long long cap)
 
 size_t transient_bytes(int NS, bool mixed, long long cap)
 {
-    if (mixed) return (size_t)2 * NS * 4 * cap + 4 * 256;
-    return (size_t)2 * NS * 8 * cap + 4 * 256;
+    if (mixed) return (size_t)2 * NS * 4 * cap + (size_t)4 * cap + 4 * 256;
+    return (size_t)2 * NS * 8 * cap + (size_t)4 * cap + 4 * 256;
 }
 
 void assign_persistent(DevState& S, void* block, int NS, bool mixed, long long cap)
@@ -137,6 +137,7 @@ void assign_transient(DevState& S, void* block, int NS, bool mixed, long long ca
         S.acc = carve<double>(p, (long long)NS * cap);
         S.k32 = S.ksum32 = nullptr;
     }
+    S.rslot = carve<int>(p, cap);
 }
 
 void free_graphs(emu_context* c)

@@ -41,6 +41,11 @@ struct DevState {
     float* vhat32[3] = {};
     float* N32[2] = {};
     long long* id = nullptr;
+    // slot of each particle in its CTA's key-ranked deposit order (a
+    // permutation of each 128-particle tile's active slots): the rank the
+    // last stage 4 computed for the new positions, which stages 1-3 of the
+    // next step deposit at; identity after a load or a re-sort
+    int* rslot = nullptr;
 };
 
 // Device-side step control: the timestep, time and error state live on the

@@ -499,9 +499,13 @@ __device__ __forceinline__ bool distinct_key_rank(int key, int* scratch, int& sl
 // end of a step): the 128 keys are ranked first (stable, so cell-sorted
 // particles keep their order), so that each stencil forms one run
 // COMB: the mixed path's combined deposit (fN holds the NF^2 combinations)
+// given_slot >= 0 (in every thread, or in none): the record slots are given
+// (a rank made earlier for the same keys) and no ranking is done.  Returns
+// the thread's slot.
 template <int NF, class SWt, class R, class T, class Conv, bool COMB = false>
-__device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
-                                                   const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false)
+__device__ __forceinline__ int tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
+                                                  const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false,
+                                                  int given_slot = -1)
 {
     using Sort = cub::BlockRadixSort<unsigned, kBlock, 1, int>;
     static_assert(sizeof(typename Sort::TempStorage) <= kBlock * TileRec<NF, SWt, R>::RW * sizeof(R),
@@ -514,7 +518,9 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
     R* srec = reinterpret_cast<R*>(tile_smem + kBlock * 8);
     const int key = active ? stencil_key(P, st.b) : -1;
     int slot = threadIdx.x;
-    if (sort_keys) {
+    if (given_slot >= 0) {
+        slot = given_slot;
+    } else if (sort_keys) {
         // rank the keys (scratch in the record area, not yet written), then
         // every thread writes its record at its key's rank
         if (distinct_key_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), slot)) {
@@ -538,6 +544,7 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
         __syncthreads();
         tile_deposit<NF, kBlock, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
     }
+    return slot;
 }
 
 // The same for a species-split CTA (kBlock particles, 2 kBlock threads:
@@ -545,9 +552,9 @@ __device__ __forceinline__ void tile_deposit_block(const DevParams& P, T* mesh, 
 // of a particle write their species' f N into its record; the species-0
 // thread writes the key, weights and velocity.
 template <int NF, class SWt, class R, class T, class Conv>
-__device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* mesh, bool active,
-                                                         const Stencil<R>& st, int sp, const R* fNs, R vx, R vy, R vz,
-                                                         Conv conv, bool sort_keys)
+__device__ __forceinline__ int tile_deposit_block_split(const DevParams& P, T* mesh, bool active,
+                                                        const Stencil<R>& st, int sp, const R* fNs, R vx, R vy, R vz,
+                                                        Conv conv, bool sort_keys, int given_slot = -1)
 {
     using TR = TileRec<NF, SWt, R>;
     constexpr int NT = 2 * kBlock, NH = NF * NF, RW = TR::RW, SP = TR::SP;
@@ -561,7 +568,9 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
     const int pl = threadIdx.x % kBlock;
     const int key = active ? stencil_key(P, st.b) : -1;
     int slot = pl;
-    if (sort_keys) {
+    if (given_slot >= 0) {
+        slot = given_slot;
+    } else if (sort_keys) {
         int sl = pl;
         if (distinct_key_rank<kBlock / 32>(key, reinterpret_cast<int*>(srec), sl)) {
             // the species-0 threads (the first kBlock) hold the ranks
@@ -597,6 +606,7 @@ __device__ __forceinline__ void tile_deposit_block_split(const DevParams& P, T* 
     for (int e = 0; e < NH; e++) r[SP + sp * NH + e] = fNs[e];
     __syncthreads();
     tile_deposit<NF, NT, kBlock, SWt, R, T>(P, mesh, skey, srec, kBlock, conv);
+    return slot;
 }
 
 // ===========================================================================
@@ -740,9 +750,14 @@ __device__ __forceinline__ void rk4_stage_body(const DevParams& P, const DevStat
             make_stencil<double>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    if (mesh_out)   // (null: the stage-4 deposit is made by the re-sort gather)
-        tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
-                                            [](double a, int) -> double { return a; }, s == 4 || P.rank_stages);
+    if (mesh_out) {   // (null: the stage-4 deposit is made by the re-sort gather)
+        // stages 1-3 deposit at the step-start positions: the rank stage 4
+        // stored for them (identity after a load or re-sort)
+        const int given = (s < 4 && P.rank_stages) ? (active ? S.rslot[p] : (int)threadIdx.x) : -1;
+        const int sl = tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
+                                                           [](double a, int) -> double { return a; }, s == 4, given);
+        if (s == 4 && active) S.rslot[p] = sl;
+    }
 }
 
 // FP64 potential of one species (potential_fp64 restricted to species sp)
@@ -867,9 +882,14 @@ __device__ __forceinline__ void rk4_stage_body_split(const DevParams& P, const D
             make_stencil<double>(P, xn[0], xn[1], xn[2], st);
         }
     }
-    if (mesh_out)
-        tile_deposit_block_split<NF, SWt, double>(P, mesh_out, active, st, sp, fN, vx, vy, vz,
-                                                  [](double a, int) -> double { return a; }, s == 4 || P.rank_stages);
+    if (mesh_out) {
+        // (stages 1-3: the rank the last stage 4 stored, see rk4_stage_body)
+        const int given = (s < 4 && P.rank_stages) ? (active ? S.rslot[p] : (int)(threadIdx.x % kBlock)) : -1;
+        const int sl = tile_deposit_block_split<NF, SWt, double>(P, mesh_out, active, st, sp, fN, vx, vy, vz,
+                                                                 [](double a, int) -> double { return a; }, s == 4,
+                                                                 given);
+        if (s == 4 && active && sp == 0) S.rslot[p] = sl;
+    }
 }
 
 // Two flavors, 1D stencils: species-split kernels (2 kBlock threads per
@@ -1441,17 +1461,20 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         __syncthreads();
     }
     if (qout) {
+        // (stages 1-3: the rank the last stage 4 stored, see rk4_stage_body)
+        const int given = (s < 4 && P.rank_stages) ? (active ? S.rslot[p] : t) : -1;
         if (s == 3) {
             // M_4, the mesh compute_dt reads (N, Nbar and the fluxes apart):
             // the full layout
-            tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, P.rank_stages != 0);
+            tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, false, given);
         } else {
             // M_2, M_3 and the next step's M_1: only the combinations the
             // stages interpolate
             float cN[NH];
             combine_species<NF>(fN, cN);
-            tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(P, qout, active, st, cN, vx, vy, vz,
-                                                                            QuantConvG{P}, s == 4 || P.rank_stages);
+            const int sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(
+                P, qout, active, st, cN, vx, vy, vz, QuantConvG{P}, s == 4, given);
+            if (s == 4 && active) S.rslot[p] = sl;
         }
     }
 }
@@ -1469,6 +1492,7 @@ __global__ void k_pack(DevParams P, const double* __restrict__ aos, const unsign
     if (i >= n) return;
     const long long row = perm ? (long long)perm[i] : i;
     const double* r = aos + row * NR;
+    S.rslot[i] = (int)(i % kBlock);   // cell-sorted: the identity rank
     for (int d = 0; d < 3; d++) S.pos[d][i] = r[d];
     S.time[i] = r[3 + 0];
     for (int d = 0; d < 4; d++) S.pup[d][i] = r[3 + 4 + d];
@@ -1551,6 +1575,7 @@ __global__ void k_gather_state(DevState src, DevState dst, const unsigned* __res
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= src.n) return;
     const long long j = perm[i];
+    dst.rslot[i] = (int)(i % kBlock);   // re-sorted: the identity rank
     for (int d = 0; d < 3; d++) { dst.pos[d][i] = src.pos[d][j]; dst.vhat[d][i] = src.vhat[d][j]; }
     dst.time[i] = src.time[j];
     for (int d = 0; d < 4; d++) dst.pup[d][i] = src.pup[d][j];
@@ -1583,6 +1608,7 @@ __global__ void __launch_bounds__(kBlock) k_gather_deposit(DevParams P, DevState
     R vx = 0, vy = 0, vz = 0;
     if (active) {
         const long long j = perm[i];
+        dst.rslot[i] = (int)(i % kBlock);   // re-sorted: the identity rank
         double x[3];
         for (int d = 0; d < 3; d++) {
             x[d] = src.pos[d][j];
