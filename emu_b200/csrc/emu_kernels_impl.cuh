@@ -329,8 +329,9 @@ __device__ __forceinline__ void dt_reduce_and_finish(const DevParams& P, const T
     constexpr int NH = NF * NF, ND = 8 * NH;
     double va = 0.0, vs = 0.0;
     if (P.flavor_cfl_factor > 0.0 && blockIdx.x < ncb) {
+        // cell c goes to block c % ncb: every block takes a few cells
         const long long stride = (long long)ncb * blockDim.x;
-        for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < P.ncells; c += stride) {
+        for (long long c = blockIdx.x + (long long)ncb * threadIdx.x; c < P.ncells; c += stride) {
             const T* m = mesh + c * ND;
             double a, b;
             cell_potentials<NF>(P, [&](int q) { return mesh_value<T>(P, m, q, NH); }, a, b);
@@ -356,9 +357,12 @@ __device__ __forceinline__ void dt_reduce_and_finish(const DevParams& P, const T
     }
 }
 
+// blocks of a stage grid that take part in the compute_dt cell reduction:
+// 32 cells per block (one per thread of a warp's worth), at most 1184 blocks
+// (each adds its maxima with two atomics on the same words)
 __device__ __forceinline__ unsigned reduce_blocks(const DevParams& P)
 {
-    long long g = (P.ncells + blockDim.x - 1) / blockDim.x;
+    long long g = (P.ncells + 31) / 32;
     if (g > 1184) g = 1184;
     if (g > gridDim.x) g = gridDim.x;
     return (unsigned)(g < 1 ? 1 : g);
