@@ -374,11 +374,12 @@ class Context:
     # ---- discrete adjoint (FP64 RK4) ----
     def adjoint_reserve(self, nsteps, checkpoint_interval):
         """Allocate a recorded run's storage up front; returns (device bytes,
-        stage states stored per segment, sub-checkpoint spacing or 0)."""
+        stage-state storage: 2 every step of the run (no recompute), 1 per
+        segment, 0 per step; sub-checkpoint spacing or 0)."""
         b, st, sub = ctypes.c_int64(0), ctypes.c_int(0), ctypes.c_int(0)
         self._ck(self.lib.emu_adjoint_reserve(self.h, int(nsteps), int(checkpoint_interval), ctypes.byref(b),
                                               ctypes.byref(st), ctypes.byref(sub)), "emu_adjoint_reserve")
-        return int(b.value), bool(st.value), int(sub.value)
+        return int(b.value), int(st.value), int(sub.value)
 
     def adjoint_forward(self, nsteps, checkpoint_interval, start_time=0.0):
         """Recorded run of nsteps from the loaded state; returns (dts, info)."""

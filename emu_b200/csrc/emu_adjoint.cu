@@ -50,6 +50,11 @@ struct emu_adjoint {
     bool recorded = false;
     bool store = false;         // stage states of a whole segment fit (else one step at a time)
     int sub = 0;                // per-step mode: sub-checkpoint spacing inside a segment (0: none)
+    // the whole run's step states, stage states and meshes fit: the recorded
+    // forward stores them (cooperative segment kernel computing dt on the
+    // device) and the backward recomputes nothing; full_steps = capacity
+    bool full = false;
+    int full_steps = 0;
     double t0 = 0.0;
     std::vector<double> dts;
     std::vector<char> resorted; // segment c began with a cell re-sort (permutation perm[c])
@@ -396,7 +401,7 @@ __device__ __forceinline__ void adj_fwd_stage4_next_body(const DevParams& P, con
                                                          const double* __restrict__ Y4, const double* __restrict__ acc,
                                                          double* __restrict__ Yn, double* __restrict__ Ynext,
                                                          double* __restrict__ xnext, const double* __restrict__ mesh_in,
-                                                         double* __restrict__ mesh_next)
+                                                         double* __restrict__ mesh_next, StepCtl* report = nullptr)
 {
     constexpr int NH = NF * NF, NS = 2 * NH;
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,6 +419,7 @@ __device__ __forceinline__ void adj_fwd_stage4_next_body(const DevParams& P, con
         double V[NS];
         potential_fp64<NF, SWt>(P, mesh_in, st, vx, vy, vz, S.vscale[p], V);
         const double bw = dt * kRK4B[3];
+        int stt = 0;
 #pragma unroll
         for (int sp = 0; sp < 2; sp++) {
             double f[NH], K[NH];
@@ -427,7 +433,7 @@ __device__ __forceinline__ void adj_fwd_stage4_next_body(const DevParams& P, con
                 Yn[o] = f[e];
             }
             if (Ynext) {
-                renormalize<NF>(f, S.Ll[sp][p], P.maxError);
+                stt |= renormalize<NF>(f, S.Ll[sp][p], P.maxError);
                 const double Ns = S.Nn[sp][p];
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
@@ -452,6 +458,7 @@ __device__ __forceinline__ void adj_fwd_stage4_next_body(const DevParams& P, con
             }
             make_stencil<double>(P, xn[0], xn[1], xn[2], st);
         }
+        if (report) report_bad(report, stt, S.id[p]);
     }
     if (mesh_next)
         tile_deposit_block<NF, SWt, double>(P, mesh_next, active, st, fN, vx, vy, vz,
@@ -481,6 +488,8 @@ struct SegPtrs {
     double* mst;
     long long mst_stride;
     const double* dts;
+    double* dts_out;   // record: the forward run itself, dt from the device step control, stored here
+    int record;
     int k0, len, NS;
     double* acc;
     double* lm[4];
@@ -540,7 +549,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
 #pragma unroll 1
     for (int j = 0; j < G.len; j++) {
         const DevState Q = seg_state(S, G, j);
-        const double dt = G.dts[G.k0 + j];
+        // recording: this step's dt from the device control (every block
+        // reads it before any block can reach the reduction that replaces it)
+        const double dt = G.record ? __ldcg(&ctl->dt) : G.dts[G.k0 + j];
+        if (G.record && blockIdx.x == 0 && threadIdx.x == 0) G.dts_out[G.k0 + j] = dt;
         const double* Y0 = seg_f(G, j);
 #pragma unroll 1
         for (int s = 1; s <= 3; s++) {
@@ -548,13 +560,38 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
                                         seg_y(G, j, s + 1, cap), seg_m(G, j, s - 1), seg_m(G, j, s));
             grid_barrier(ctl);
         }
-        const bool more = j + 1 < G.len;
+        // (recording: the state after the segment goes to slot len too)
+        const bool more = j + 1 < G.len, next = more || G.record;
         adj_fwd_stage4_next_body<NF, SWt>(P, Q, dt, seg_y(G, j, 4, cap), G.acc, seg_y(G, j, 5, cap),
-                                          more ? seg_f(G, j + 1) : nullptr,
-                                          more ? seg_f(G, j + 1) + (long long)G.NS * cap : nullptr, seg_m(G, j, 3),
-                                          more ? seg_m(G, j + 1, 0) : nullptr);
+                                          next ? seg_f(G, j + 1) : nullptr,
+                                          next ? seg_f(G, j + 1) + (long long)G.NS * cap : nullptr, seg_m(G, j, 3),
+                                          more ? seg_m(G, j + 1, 0) : nullptr, G.record ? ctl : nullptr);
         grid_barrier(ctl);
+        if (G.record) {
+            // compute_dt on the stage-4 mesh (main.cpp:193-198): the next dt
+            dt_reduce_and_finish<NF, double>(P, seg_m(G, j, 3), ctl, DT_ADVANCE, reduce_blocks(P));
+            grid_barrier(ctl);
+            if (__ldcg(&ctl->done) && more) break;   // (uniform: read after the barrier)
+        }
     }
+}
+
+// particle time of a recorded segment: time += dt_j * b_i, stage by stage and
+// step by step, in the order of the step kernels
+__global__ void k_time_advance(DevState S, const double* __restrict__ dts, int k0, int len)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    double tn = S.time[p];
+    for (int j = 0; j < len; j++) {
+        const double dt = dts[k0 + j];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const double w = dt * kRK4B[i];
+            tn = __dadd_rn(w, tn);
+        }
+    }
+    S.time[p] = tn;
 }
 
 // Backward over a whole segment in one cooperative launch: five phases per
@@ -770,6 +807,11 @@ bool adj_coop_fits(int nf, const DevParams& P, long long n)
     return nf == 2 && adj_coop_fits_t<2>(P, n);
 }
 
+void launch_time_advance(const DevState& S, const double* dts, int k0, int len, cudaStream_t st)
+{
+    k_time_advance<<<grid_for(S.n), kBlock, 0, st>>>(S, dts, k0, len);
+}
+
 cudaError_t launch_adj_seg_coop(int nf, bool forward, const DevParams& P, const DevState& S, const SegPtrs& G,
                                 StepCtl* ctl, cudaStream_t st)
 {
@@ -861,7 +903,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
     const long long nm = mesh_elems(ctx);
     emu_adjoint* a = ctx->adj;
     if (a && (a->cap != cap || a->NS != NS || a->ck_slots < nck || a->interval_cap < interval ||
-              (int)a->dts.size() < nsteps)) {
+              (int)a->dts.size() < nsteps || (a->full && a->full_steps < nsteps))) {
         free_adj(a);
         a = ctx->adj = nullptr;
     }
@@ -884,13 +926,18 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         if (const char* env = std::getenv("EMU_ADJOINT_STORE_MAX_BYTES")) budget = (size_t)std::strtoull(env, nullptr, 10);
         const size_t per_step = sizeof(double) * ((size_t)4 * NS * cap + (size_t)4 * nm);
         a->store = (size_t)interval * per_step <= budget;
-        const size_t st_steps = a->store ? (size_t)interval : 1;
+        const char* fenv = std::getenv("EMU_ADJOINT_FULL_STORE");
+        a->full = a->store && (!fenv || std::atoi(fenv) != 0) &&
+                  emu::adj_coop_fits(ctx->nf, ctx->P, ctx->S[ctx->cur].n) &&
+                  (size_t)nsteps * (per_step + sizeof(double) * slot) <= budget;
+        a->full_steps = a->full ? nsteps : 0;
+        const size_t st_steps = a->full ? (size_t)nsteps : a->store ? (size_t)interval : 1;
         // per-step mode: the states of every step of a segment (interval
         // slots), or, when the checkpoints and those slots would not fit in
         // the free memory, sub-checkpoints every J ~ sqrt(interval) steps
         // (J + interval / J slots; each step is recomputed once more)
         a->sub = 0;
-        a->seg_slots = interval;
+        a->seg_slots = a->full ? nsteps + 1 : interval;
         if (!a->store) {
             const size_t other = sizeof(double) * ((size_t)st_steps * 4 * (NS * cap + nm) + (size_t)(6 * NS + 8) * cap +
                                                    (size_t)4 * nm + (size_t)NS * cap + 2 * 13 * cap) +
@@ -1007,6 +1054,64 @@ int segment_sweep(emu_context* ctx, const DevState& W, const emu::SegPtrs& G, bo
     return check_launch(ctx, "adjoint segment");
 }
 
+// The recorded forward run when every step's states fit (a->full): per
+// segment a cell re-sort at its start (as the step loop), then one
+// cooperative launch that advances the segment with dt from the device step
+// control, storing Y_0 and x, the stage states and the meshes of every step
+// (what the backward would otherwise recompute), then the particle time and
+// the state after the segment back into the context.
+int record_full(emu_context* ctx, emu_adjoint* a, int nsteps, int interval)
+{
+    const int NS = ctx->NS;
+    const long long cap = ctx->cap, nm = mesh_elems(ctx);
+    cudaStream_t st = ctx->stream;
+    int r;
+    emu::SegPtrs G{};
+    G.seg_stride = (long long)(NS + 3) * cap;
+    G.sst_stride = (long long)4 * NS * cap;
+    G.mst_stride = 4 * nm;
+    G.dts = a->dts_dev;
+    G.dts_out = a->dts_dev;
+    G.record = 1;
+    G.NS = NS;
+    G.acc = a->acc;
+    G.nmesh = nm;
+    const int nseg = (nsteps + interval - 1) / interval;
+    for (int c = 0; c < nseg; c++) {
+        const int k0 = c * interval, len = std::min(k0 + interval, nsteps) - k0;
+        if (c > 0 && ctx->prm.resort_interval > 0) {
+            if ((r = emu_ctx::resort_now(ctx, a->perm + (size_t)c * a->cap))) return r;
+            a->resorted[c] = 1;
+        }
+        const DevState& S = ctx->S[ctx->cur];
+        if ((r = save_slot(ctx, a, a->ck, c, S.f0, S.pos))) return r;
+        if ((r = save_slot(ctx, a, a->seg, k0, S.f0, S.pos))) return r;
+        G.seg = a->seg + (size_t)k0 * G.seg_stride;
+        G.sst = a->sst + (size_t)k0 * G.sst_stride;
+        G.mst = a->mst + (size_t)k0 * G.mst_stride;
+        G.k0 = k0;
+        G.len = len;
+        CU(cudaMemsetAsync(G.mst, 0, sizeof(double) * (size_t)len * 4 * nm, st));
+        if ((r = deposit_into(ctx, emu::seg_state(S, G, 0), emu::seg_f(G, 0), emu::seg_m(G, 0, 0)))) return r;
+        cudaError_t e = emu::launch_adj_seg_coop(ctx->nf, true, ctx->P, S, G, ctx->ctl, st);
+        if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("recorded segment: ") + cudaGetErrorString(e));
+        emu::launch_time_advance(S, a->dts_dev, k0, len, st);
+        CU(cudaMemcpyAsync(S.f0, emu::seg_f(G, len), sizeof(double) * (size_t)NS * cap, cudaMemcpyDeviceToDevice, st));
+        for (int d = 0; d < 3; d++)
+            CU(cudaMemcpyAsync(S.pos[d], emu::seg_f(G, len) + (size_t)(NS + d) * cap, sizeof(double) * cap,
+                               cudaMemcpyDeviceToDevice, st));
+        if ((r = check_launch(ctx, "recorded segment"))) return r;
+    }
+    // the context as after the step loop: the new state's deposit in mesh 0,
+    // the last step's stage-4 mesh as the current mesh
+    if ((r = deposit_into(ctx, ctx->S[ctx->cur], ctx->S[ctx->cur].f0, ctx->mesh[0]))) return r;
+    CU(cudaMemsetAsync(ctx->mesh[1], 0, sizeof(double) * nm, st));
+    CU(cudaMemcpyAsync(ctx->mesh[3], a->mst + (size_t)(nsteps - 1) * G.mst_stride + 3 * nm, sizeof(double) * nm,
+                       cudaMemcpyDeviceToDevice, st));
+    ctx->cur_mesh = 3;
+    return EMU_OK;
+}
+
 }  // namespace
 
 void emu_ctx::adjoint_free(emu_context* ctx)
@@ -1028,7 +1133,7 @@ int emu_adjoint_reserve(emu_context* ctx, int nsteps, int checkpoint_interval, i
     if ((r = ensure_adj(ctx, nsteps, checkpoint_interval))) return r;
     const emu_adjoint* a = ctx->adj;
     if (device_bytes) *device_bytes = (int64_t)a->bytes;
-    if (stage_store) *stage_store = a->store ? 1 : 0;
+    if (stage_store) *stage_store = a->full ? 2 : a->store ? 1 : 0;
     if (sub_interval) *sub_interval = a->sub;
     return EMU_OK;
 }
@@ -1049,6 +1154,9 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
     a->t0 = start_time;
     std::fill(a->resorted.begin(), a->resorted.end(), 0);
     if ((r = emu_evolve_begin(ctx, start_time, INFINITY, nsteps))) return r;
+    if (a->full) {
+        if ((r = record_full(ctx, a, nsteps, checkpoint_interval))) return r;
+    } else {
     emu::launch_ctl_hist(ctx->ctl, a->dts_dev, ctx->stream);   // the step kernels record their dt
     for (int k = 0; k < nsteps; k++) {
         if (k % checkpoint_interval == 0) {
@@ -1065,6 +1173,7 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
         if ((r = emu_ctx::step_device(ctx))) return r;
     }
     emu::launch_ctl_hist(ctx->ctl, nullptr, ctx->stream);
+    }
     ctx->steps_since_sort = 0;
     emu_run_info ri{};
     r = emu_evolve_end(ctx, &ri);
@@ -1179,7 +1288,18 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
         DevState W = stat_view(a, w, S);   // static fields in this segment's slot order
         W.fs = S.fs;
         W.acc = S.acc;
-        if (a->store) {
+        if (a->full) {
+            // the recorded forward stored every step: only the sweep
+            G.seg = a->seg + (size_t)k0 * G.seg_stride;
+            G.sst = a->sst + (size_t)k0 * G.sst_stride;
+            G.mst = a->mst + (size_t)k0 * G.mst_stride;
+            G.k0 = k0;
+            G.len = len;
+            cudaError_t e = emu::launch_adj_seg_coop(nf, false, ctx->P, W, G, ctx->ctl, st);
+            if (e != cudaSuccess)
+                return fail(ctx, EMU_ERR_CUDA, std::string("adjoint segment: ") + cudaGetErrorString(e));
+            if ((r = check_launch(ctx, "adjoint segment"))) return r;
+        } else if (a->store) {
             G.seg = a->seg;
             G.k0 = k0;
             G.len = len;

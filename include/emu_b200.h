@@ -266,7 +266,11 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * (lam_f_final, n x 2nf^2) and optionally dJ/d(N, Nbar) taken at the final
  * state (lam_N_final, n x 2, NULL = 0), the gradient with respect to the
  * run's initial f (lam_f0) and N, Nbar (lam_N0), with the recorded dt held
- * fixed.  Recomputes each checkpoint segment from its checkpoint; the stage
+ * fixed.  When the states, stage states and meshes of every step of the run
+ * fit the budget below (and, two flavors, the grid is co-resident), the
+ * recorded forward stores them and the backward recomputes nothing
+ * (environment variable EMU_ADJOINT_FULL_STORE=0 turns this off).  Otherwise
+ * it recomputes each checkpoint segment from its checkpoint; the stage
  * states and meshes of a whole segment are kept when they fit a budget
  * (a quarter of the free device memory, at most 16 GiB; environment variable
  * EMU_ADJOINT_STORE_MAX_BYTES overrides it), else each step's stages are
@@ -281,9 +285,10 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * emu_adjoint_reserve: allocates the checkpoint and work storage of a
  * recorded run of nsteps with this checkpoint_interval up front (what
  * emu_adjoint_forward would allocate), so that a timed or repeated run does
- * no allocation.  Optional outputs: the device bytes held, whether stage
- * states of whole segments are stored (1) or recomputed per step (0), and
- * the sub-checkpoint spacing (0 = none).
+ * no allocation.  Optional outputs: the device bytes held, how stage states
+ * are kept (2: every step of the run, stored by the recorded forward; 1:
+ * recomputed and kept per segment; 0: recomputed per step), and the
+ * sub-checkpoint spacing (0 = none).
  */
 /*
  * Particle sharding over GPUs (one process per GPU).  No counterpart in the

@@ -151,13 +151,16 @@ def test_adjoint_errors():
             c.adjoint_forward(3, 2)
 
 
-@pytest.mark.parametrize("store", ["segment", "per_step", "per_step_sub2", "per_step_sub3"])
+@pytest.mark.parametrize("store", ["full", "segment", "per_step", "per_step_sub2", "per_step_sub3"])
 def test_adjoint_memory_modes_agree(monkeypatch, store):
-    """stage states kept for a whole segment, recomputed step by step
-    (budget 0), or step by step from sub-checkpoints every 2 or 3 steps
-    inside a 7-step segment (the mode for runs whose checkpoints and step
-    states would not fit in memory): same gradient to rounding"""
-    if store != "segment":
+    """every step stored by the recorded forward (no recompute), stage states
+    recomputed and kept for a whole segment, recomputed step by step (budget
+    0), or step by step from sub-checkpoints every 2 or 3 steps inside a
+    7-step segment (the mode for runs whose checkpoints and step states would
+    not fit in memory): same gradient to rounding"""
+    if store == "segment":
+        monkeypatch.setenv("EMU_ADJOINT_FULL_STORE", "0")
+    elif store != "full":
         monkeypatch.setenv("EMU_ADJOINT_STORE_MAX_BYTES", "0")
     if store.startswith("per_step_sub"):
         monkeypatch.setenv("EMU_ADJOINT_SUBCHECKPOINT", store[-1])
@@ -165,6 +168,9 @@ def test_adjoint_memory_modes_agree(monkeypatch, store):
     parts = api.init_particles(p)
     fc, nc = flavor_columns(2), number_columns(2)
     with AdjointRun(p, parts, 16, 7) as run:
+        run.load(parts[:, fc], parts[:, nc])
+        nbytes, stage_store, sub = run.ctx.adjoint_reserve(16, 7)
+        assert stage_store == {"full": 2, "segment": 1}.get(store, 0)
         run.forward(parts[:, fc], parts[:, nc])
         J, lf, lN = run.ctx.adjoint_objective()
         g, gN = run.ctx.adjoint_backward(lf, lN)
