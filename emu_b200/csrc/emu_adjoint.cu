@@ -560,6 +560,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
                                         seg_y(G, j, s + 1, cap), seg_m(G, j, s - 1), seg_m(G, j, s));
             grid_barrier(ctl);
         }
+        // recording: compute_dt on the stage-4 mesh (main.cpp:193-198), the
+        // next step's dt; M_4 is complete and every block holds this step's
+        // dt, so it overlaps stage 4 and shares its barrier
+        if (G.record) dt_reduce_and_finish<NF, double>(P, seg_m(G, j, 3), ctl, DT_ADVANCE, reduce_blocks(P));
         // (recording: the state after the segment goes to slot len too)
         const bool more = j + 1 < G.len, next = more || G.record;
         adj_fwd_stage4_next_body<NF, SWt>(P, Q, dt, seg_y(G, j, 4, cap), G.acc, seg_y(G, j, 5, cap),
@@ -567,12 +571,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
                                           next ? seg_f(G, j + 1) + (long long)G.NS * cap : nullptr, seg_m(G, j, 3),
                                           more ? seg_m(G, j + 1, 0) : nullptr, G.record ? ctl : nullptr);
         grid_barrier(ctl);
-        if (G.record) {
-            // compute_dt on the stage-4 mesh (main.cpp:193-198): the next dt
-            dt_reduce_and_finish<NF, double>(P, seg_m(G, j, 3), ctl, DT_ADVANCE, reduce_blocks(P));
-            grid_barrier(ctl);
-            if (__ldcg(&ctl->done) && more) break;   // (uniform: read after the barrier)
-        }
+        if (G.record && __ldcg(&ctl->done) && more) break;   // (uniform: read after the barrier)
     }
 }
 
