@@ -325,7 +325,10 @@ def run_emu(args):
     if not args.no_e2e:
         import threading
         # (pinned host buffers of all batches within 32 GB)
-        pipes = max(1, min(args.e2e_pipes, int(32e9 // (2 * recs.nbytes)))) if ws == 1 else 1
+        # (automatic: 16 small batches in flight, 8 large ones, whose copies
+        # already fill PCIe and contend beyond that)
+        want = args.e2e_pipes if args.e2e_pipes > 0 else (16 if recs.nbytes < 16e6 else 8)
+        pipes = max(1, min(want, int(32e9 // (2 * recs.nbytes)))) if ws == 1 else 1
         ne = min(args.steps, args.e2e_steps)
         lanes = []
         for k in range(pipes):
@@ -493,8 +496,9 @@ def main():
                     help="particle-sharded path even on one GPU (a one-rank communicator)")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--e2e-pipes", type=int, default=8,
-                    help="batches in flight for the end-to-end figure (one GPU)")
+    ap.add_argument("--e2e-pipes", type=int, default=0,
+                    help="batches in flight for the end-to-end figure (one GPU; 0 = 16 for batches under "
+                         "16 MB, else 8)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--adjoint", action="store_true",
