@@ -75,6 +75,7 @@ struct emu_adjoint {
     double *acc = nullptr, *lamY0 = nullptr, *lamN = nullptr, *lamn = nullptr, *lamYd = nullptr;
     double *wf = nullptr, *lamtmp = nullptr, *wpos = nullptr, *wtime = nullptr;
     double* rows = nullptr;     // n x NS staging for host transfers
+    unsigned* map[2] = {};      // recorded forward: slot -> slot at the segment start, through the re-sorts
 };
 
 namespace emu {
@@ -575,6 +576,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
     }
 }
 
+// composition of a re-sort (new slot i holds old slot g[i]) into the map of
+// slots to segment-start slots
+__global__ void k_compose_map(const unsigned* __restrict__ map_old, const unsigned* __restrict__ g,
+                              unsigned* __restrict__ map_new, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) map_new[i] = map_old ? map_old[g[i]] : g[i];
+}
+
 // particle time of a recorded segment: time += dt_j * b_i, stage by stage and
 // step by step, in the order of the step kernels
 __global__ void k_time_advance(DevState S, const double* __restrict__ dts, int k0, int len)
@@ -806,6 +816,11 @@ bool adj_coop_fits(int nf, const DevParams& P, long long n)
     return nf == 2 && adj_coop_fits_t<2>(P, n);
 }
 
+void launch_compose_map(const unsigned* map_old, const unsigned* g, unsigned* map_new, long long n, cudaStream_t st)
+{
+    k_compose_map<<<grid_for(n), kBlock, 0, st>>>(map_old, g, map_new, n);
+}
+
 void launch_time_advance(const DevState& S, const double* dts, int k0, int len, cudaStream_t st)
 {
     k_time_advance<<<grid_for(S.n), kBlock, 0, st>>>(S, dts, k0, len);
@@ -867,7 +882,7 @@ void free_adj(emu_adjoint* a)
 {
     if (!a) return;
     for (void* p : {(void*)a->dts_dev, (void*)a->ck, (void*)a->seg, (void*)a->work, (void*)a->nex, (void*)a->rows,
-                    (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst})
+                    (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst, (void*)a->map[0], (void*)a->map[1]})
         if (p) cudaFree(p);
     for (int i = 0; i < 4; i++)
         if (a->lmesh[i]) cudaFree(a->lmesh[i]);
@@ -967,6 +982,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         for (int i = 0; i < 4; i++) CU(alloc(&a->lmesh[i], sizeof(double) * nm));
         CU(alloc(&a->nex, sizeof(double) * 2 * ctx->P.ncells));
         CU(alloc(&a->rows, sizeof(double) * (size_t)NS * cap));
+        for (int i = 0; i < 2; i++) CU(alloc(&a->map[i], sizeof(unsigned) * cap));
         double* w = a->work;
         a->acc = w; w += (size_t)NS * cap;
         a->lamY0 = w; w += (size_t)NS * cap;
@@ -1157,19 +1173,32 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
         if ((r = record_full(ctx, a, nsteps, checkpoint_interval))) return r;
     } else {
     emu::launch_ctl_hist(ctx->ctl, a->dts_dev, ctx->stream);   // the step kernels record their dt
+    // cell re-sorts on the step loop's schedule; the backward recomputes each
+    // segment in its start order, so a segment's re-sorts are composed into
+    // one map (slot -> slot at the segment start) that the backward undoes at
+    // the next boundary
+    int nmap = 0, mcur = 0;
+    const long long n = ctx->S[ctx->cur].n;
     for (int k = 0; k < nsteps; k++) {
         if (k % checkpoint_interval == 0) {
             const int c = k / checkpoint_interval;
-            // cell re-sort at segment starts only: the order is fixed inside a
-            // segment; the backward undoes the permutation at the boundary
-            if (c > 0 && ctx->prm.resort_interval > 0) {
-                if ((r = emu_ctx::resort_now(ctx, a->perm + (size_t)c * a->cap))) return r;
+            if (c > 0 && nmap > 0) {
+                CU(cudaMemcpyAsync(a->perm + (size_t)c * a->cap, a->map[mcur], sizeof(unsigned) * n,
+                                   cudaMemcpyDeviceToDevice, ctx->stream));
                 a->resorted[c] = 1;
             }
+            nmap = 0;
             const DevState& S = ctx->S[ctx->cur];
             if ((r = save_slot(ctx, a, a->ck, c, S.f0, S.pos))) return r;
         }
         if ((r = emu_ctx::step_device(ctx))) return r;
+        const int ri = ctx->prm.resort_interval;
+        if (ri > 0 && k + 1 < nsteps && (k + 1) % ri == 0) {
+            if ((r = emu_ctx::resort_now(ctx, nullptr))) return r;
+            emu::launch_compose_map(nmap ? a->map[mcur] : nullptr, ctx->idx2, a->map[1 - mcur], n, ctx->stream);
+            mcur = 1 - mcur;
+            nmap++;
+        }
     }
     emu::launch_ctl_hist(ctx->ctl, nullptr, ctx->stream);
     }
