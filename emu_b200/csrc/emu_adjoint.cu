@@ -76,6 +76,14 @@ struct emu_adjoint {
     double *wf = nullptr, *lamtmp = nullptr, *wpos = nullptr, *wtime = nullptr;
     double* rows = nullptr;     // n x NS staging for host transfers
     unsigned* map[2] = {};      // recorded forward: slot -> slot at the segment start, through the re-sorts
+    bool final_mapped = false;  // perm slot nck: the map of the run's last segment (re-sorts in it)
+    // per-step mode with re-sorts: the backward's recompute re-sorts as the
+    // forward did; second state buffers, the re-sort permutation of every
+    // step of a sub-segment, the composed map of every sub-segment
+    double *wf2 = nullptr, *wpos2 = nullptr;
+    unsigned* gperm = nullptr;
+    unsigned* smap = nullptr;
+    int gslots = 0, sslots = 0;
 };
 
 namespace emu {
@@ -656,6 +664,32 @@ __global__ void k_static_scatter(DevState src, DevState dst, const unsigned* __r
         for (int c = 0; c < nl; c++) ldst[c * cap + j] = lsrc[c * cap + i];
 }
 
+// the same, gathering: dst[i] = src[perm[i]] (the forward direction of a re-sort)
+__global__ void k_static_gather(DevState src, DevState dst, const unsigned* __restrict__ perm)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= src.n) return;
+    const long long j = perm[i];
+    for (int d = 0; d < 3; d++) dst.vhat[d][i] = src.vhat[d][j];
+    for (int d = 0; d < 4; d++) dst.pup[d][i] = src.pup[d][j];
+    for (int sp = 0; sp < 2; sp++) {
+        dst.Nn[sp][i] = src.Nn[sp][j];
+        dst.Ll[sp][i] = src.Ll[sp][j];
+    }
+    dst.vscale[i] = src.vscale[j];
+    dst.id[i] = src.id[j];
+}
+
+// nc component arrays of stride cap: dst[c][i] = src[c][perm[i]]
+__global__ void k_rows_gather(const double* __restrict__ src, double* __restrict__ dst, const unsigned* __restrict__ perm,
+                              int nc, long long cap, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long j = perm[i];
+    for (int c = 0; c < nc; c++) dst[c * cap + i] = src[c * cap + j];
+}
+
 // objective: lam_M = 2/V_cell M on the nu e-mu components, zero elsewhere;
 // the two components per cell go to nex for the host sum
 template <int NF>
@@ -882,7 +916,8 @@ void free_adj(emu_adjoint* a)
 {
     if (!a) return;
     for (void* p : {(void*)a->dts_dev, (void*)a->ck, (void*)a->seg, (void*)a->work, (void*)a->nex, (void*)a->rows,
-                    (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst, (void*)a->map[0], (void*)a->map[1]})
+                    (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst, (void*)a->map[0], (void*)a->map[1],
+                    (void*)a->wf2, (void*)a->wpos2, (void*)a->gperm, (void*)a->smap})
         if (p) cudaFree(p);
     for (int i = 0; i < 4; i++)
         if (a->lmesh[i]) cudaFree(a->lmesh[i]);
@@ -954,8 +989,9 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         a->seg_slots = a->full ? nsteps + 1 : interval;
         if (!a->store) {
             const size_t other = sizeof(double) * ((size_t)st_steps * 4 * (NS * cap + nm) + (size_t)(6 * NS + 8) * cap +
-                                                   (size_t)4 * nm + (size_t)NS * cap + 2 * 13 * cap) +
-                                 sizeof(unsigned) * (size_t)cap * a->ck_slots;
+                                                   (size_t)4 * nm + (size_t)NS * cap + 2 * 13 * cap +
+                                                   (size_t)(NS + 3) * cap) +
+                                 sizeof(unsigned) * (size_t)cap * (a->ck_slots + 3 + 2 * (size_t)interval);
             const size_t single = sizeof(double) * slot * (size_t)(a->ck_slots + interval) + other;
             int J = 0;
             if (single > fre / 20 * 19) J = (int)std::ceil(std::sqrt((double)interval));
@@ -973,7 +1009,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         CU(alloc(&a->dts_dev, sizeof(double) * a->dts.size()));
         CU(alloc(&a->ck, sizeof(double) * slot * a->ck_slots));
         CU(alloc(&a->seg, sizeof(double) * slot * a->seg_slots));
-        CU(alloc(&a->perm, sizeof(unsigned) * cap * a->ck_slots));
+        CU(alloc(&a->perm, sizeof(unsigned) * cap * (a->ck_slots + 1)));
         CU(alloc(&a->stat, (size_t)2 * 13 * 8 * cap));
         CU(alloc(&a->sst, sizeof(double) * st_steps * 4 * NS * cap));
         CU(alloc(&a->mst, sizeof(double) * st_steps * 4 * nm));
@@ -983,6 +1019,15 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         CU(alloc(&a->nex, sizeof(double) * 2 * ctx->P.ncells));
         CU(alloc(&a->rows, sizeof(double) * (size_t)NS * cap));
         for (int i = 0; i < 2; i++) CU(alloc(&a->map[i], sizeof(unsigned) * cap));
+        if (!a->store && ctx->prm.resort_interval > 0) {
+            const int J = a->sub > 0 ? a->sub : interval;
+            a->gslots = J;
+            a->sslots = (interval + J - 1) / J;
+            CU(alloc(&a->wf2, sizeof(double) * (size_t)NS * cap));
+            CU(alloc(&a->wpos2, sizeof(double) * (size_t)3 * cap));
+            CU(alloc(&a->gperm, sizeof(unsigned) * (size_t)a->gslots * cap));
+            CU(alloc(&a->smap, sizeof(unsigned) * (size_t)a->sslots * cap));
+        }
         double* w = a->work;
         a->acc = w; w += (size_t)NS * cap;
         a->lamY0 = w; w += (size_t)NS * cap;
@@ -1168,6 +1213,7 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
     ctx->adj_valid = false;
     a->t0 = start_time;
     std::fill(a->resorted.begin(), a->resorted.end(), 0);
+    a->final_mapped = false;
     if ((r = emu_evolve_begin(ctx, start_time, INFINITY, nsteps))) return r;
     if (a->full) {
         if ((r = record_full(ctx, a, nsteps, checkpoint_interval))) return r;
@@ -1200,6 +1246,10 @@ int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, d
             nmap++;
         }
     }
+    a->final_mapped = nmap > 0;
+    if (nmap > 0)
+        CU(cudaMemcpyAsync(a->perm + (size_t)a->nck * a->cap, a->map[mcur], sizeof(unsigned) * n,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
     emu::launch_ctl_hist(ctx->ctl, nullptr, ctx->stream);
     }
     ctx->steps_since_sort = 0;
@@ -1294,6 +1344,8 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
     emu::launch_ctl_set(ctx->ctl, 0.0, 0.0, INFINITY, INT_MAX, 0, st);
     if ((r = check_launch(ctx, "adjoint input"))) return r;
     const bool coop = a->store && emu::adj_coop_fits(nf, ctx->P, n);
+    // per-step mode with re-sorts (the recomputes re-sort as the forward did)
+    const bool rps = !a->store && ctx->prm.resort_interval > 0 && a->gperm;
 
     emu::SegPtrs G{};
     G.seg_stride = (long long)(NS + 3) * cap;
@@ -1335,6 +1387,129 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
                                st));
             CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * (size_t)len * 4 * nm, st));
             if ((r = segment_sweep(ctx, W, G, coop))) return r;
+        } else if (rps) {
+            // per-step mode with re-sorts: the recomputes re-sort where the
+            // step loop did (a stable sort of the same positions gives the
+            // forward's orders), each step's permutation is kept, and the
+            // sweep undoes it on the static fields and the adjoint state
+            // before the step; W enters in the next segment's start order
+            const int ri = ctx->prm.resort_interval;
+            double* const* M = ctx->mesh;
+            const int J = (a->sub > 0 && a->sub < len) ? a->sub : len;   // steps per sub-segment
+            const int nsub = (len + J - 1) / J;
+            double *rf = a->wf, *rf2 = a->wf2, *rp = a->wpos, *rp2 = a->wpos2;
+            auto Wv = [&]() {
+                DevState V = stat_view(a, w, S);
+                V.fs = S.fs;
+                V.acc = S.acc;
+                return V;
+            };
+            auto Rv = [&]() {
+                DevState V = Wv();
+                V.f0 = rf;
+                for (int d = 0; d < 3; d++) V.pos[d] = rp + (size_t)d * cap;
+                V.time = a->wtime;
+                return V;
+            };
+            // the static fields (and with lambda the adjoint state) through a
+            // permutation: undo = scatter, else gather
+            auto move_static = [&](const unsigned* perm, bool undo, bool with_lambda) -> int {
+                const DevState src = Wv(), dst = stat_view(a, 1 - w, S);
+                if (undo)
+                    emu::k_static_scatter<<<g, emu::kBlock, 0, st>>>(src, dst, perm, with_lambda ? a->lamY0 : nullptr,
+                                                                     a->lamtmp, NS + 2);
+                else
+                    emu::k_static_gather<<<g, emu::kBlock, 0, st>>>(src, dst, perm);
+                if (undo && with_lambda)
+                    CU(cudaMemcpyAsync(a->lamY0, a->lamtmp, sizeof(double) * (size_t)(NS + 2) * cap,
+                                       cudaMemcpyDeviceToDevice, st));
+                w = 1 - w;
+                return EMU_OK;
+            };
+            // the recompute state after step k is re-sorted when the step
+            // loop re-sorted there: 1 (permutation copied to gout), 0 not due
+            auto resort_after = [&](int k, unsigned* gout, int& res) -> int {
+                res = 0;
+                if (!(k + 1 < a->nsteps && (k + 1) % ri == 0)) return EMU_OK;
+                int rr;
+                if ((rr = emu_ctx::sort_state_perm(ctx, Rv()))) return rr;
+                emu::k_rows_gather<<<g, emu::kBlock, 0, st>>>(rf, rf2, ctx->idx2, NS, cap, n);
+                emu::k_rows_gather<<<g, emu::kBlock, 0, st>>>(rp, rp2, ctx->idx2, 3, cap, n);
+                std::swap(rf, rf2);
+                std::swap(rp, rp2);
+                if ((rr = move_static(ctx->idx2, false, false))) return rr;
+                if (gout) CU(cudaMemcpyAsync(gout, ctx->idx2, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, st));
+                res = 1;
+                return EMU_OK;
+            };
+            auto restore = [&](const double* slot) -> int {
+                CU(cudaMemcpyAsync(rf, slot, sizeof(double) * NS * cap, cudaMemcpyDeviceToDevice, st));
+                CU(cudaMemcpyAsync(rp, slot + (size_t)NS * cap, sizeof(double) * 3 * cap, cudaMemcpyDeviceToDevice,
+                                   st));
+                CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
+                return deposit_into(ctx, Rv(), rf, M[0]);
+            };
+            auto advance = [&]() {
+                const DevState R = Rv();
+                for (int s = 1; s <= 4; s++)
+                    emu::launch_rk4_stage(nf, ctx->P, R, s, M[s - 1], M[s % 4], M[(s + 1) % 4], nm, ctx->ctl, -1, st);
+            };
+            const bool mapped = seg + 1 < a->nck ? a->resorted[seg + 1] != 0 : a->final_mapped;
+            if (mapped && (r = move_static(a->perm + (size_t)(seg + 1) * cap, true, false))) return r;
+            // sub-checkpoints (seg slot J + i) and the composed map of every
+            // sub-segment but the last (smap slot i: slot at sub-checkpoint
+            // i + 1 -> slot at sub-checkpoint i)
+            std::vector<int> ncomp(nsub, 0);
+            if (nsub > 1) {
+                if ((r = restore(slot_f(a, a->ck, seg)))) return r;
+                const int kl = k0 + (nsub - 1) * J;
+                int mc = 0;
+                for (int k = k0; k <= kl; k++) {
+                    const bool save = k > k0 && (k - k0) % J == 0;
+                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(
+                        Rv(), save ? slot_f(a, a->seg, J + (k - k0) / J) : nullptr, NS, a->dts_dev, k, ctx->ctl);
+                    if (k == kl) break;
+                    advance();
+                    const int i = (k - k0) / J;
+                    int res;
+                    if ((r = resort_after(k, nullptr, res))) return r;
+                    if (res) {
+                        emu::launch_compose_map(ncomp[i] ? a->map[mc] : nullptr, ctx->idx2, a->map[1 - mc], n, st);
+                        mc = 1 - mc;
+                        ncomp[i]++;
+                    }
+                    if ((k + 1 - k0) % J == 0 && ncomp[i])
+                        CU(cudaMemcpyAsync(a->smap + (size_t)i * cap, a->map[mc], sizeof(unsigned) * n,
+                                           cudaMemcpyDeviceToDevice, st));
+                }
+                if ((r = check_launch(ctx, "adjoint sub-checkpoints"))) return r;
+            }
+            for (int i = nsub - 1; i >= 0; i--) {
+                const int s0 = k0 + i * J, s1 = std::min(s0 + J, k1);
+                if (i < nsub - 1 && ncomp[i] && (r = move_static(a->smap + (size_t)i * cap, true, false))) return r;
+                if ((r = restore(i == 0 ? slot_f(a, a->ck, seg) : slot_f(a, a->seg, J + i)))) return r;
+                std::vector<int> has(s1 - s0, 0);
+                for (int k = s0; k < s1; k++) {
+                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(Rv(), slot_f(a, a->seg, k - s0), NS, a->dts_dev, k,
+                                                                ctx->ctl);
+                    const bool due = k + 1 < a->nsteps && (k + 1) % ri == 0;
+                    if (k + 1 < s1 || due) {
+                        // (the last step too when a re-sort follows it: its
+                        // permutation maps onto the next sub-segment's order)
+                        advance();
+                        if ((r = resort_after(k, a->gperm + (size_t)(k - s0) * cap, has[k - s0]))) return r;
+                    }
+                }
+                if ((r = check_launch(ctx, "adjoint segment recompute"))) return r;
+                for (int k = s1 - 1; k >= s0; k--) {
+                    if (has[k - s0] && (r = move_static(a->gperm + (size_t)(k - s0) * cap, true, true))) return r;
+                    G.seg = slot_f(a, a->seg, k - s0);
+                    G.k0 = k;
+                    G.len = 1;
+                    CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * 4 * nm, st));
+                    if ((r = segment_sweep(ctx, Wv(), G, false))) return r;
+                }
+            }
         } else {
             // (Y_0, x) of every step of a sub-segment (the whole segment
             // unless memory asked for sub-checkpoints), recomputed from the
@@ -1389,8 +1564,8 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
                 }
             }
         }
-        if (seg > 0 && a->resorted[seg]) {
-            // undo the re-sort made at the start of this segment
+        if (!rps && seg > 0 && a->resorted[seg]) {
+            // undo the re-sorts of the previous segment (composed map)
             const unsigned* perm = a->perm + (size_t)seg * cap;
             emu::k_static_scatter<<<g, emu::kBlock, 0, st>>>(W, stat_view(a, 1 - w, S), perm, a->lamY0, a->lamtmp,
                                                              NS + 2);

@@ -467,6 +467,12 @@ int emu_ctx::step_device(emu_context* ctx, bool last_stage_deposit)
     return EMU_OK;
 }
 
+int emu_ctx::sort_state_perm(emu_context* ctx, const DevState& S)
+{
+    emu::launch_state_keys(ctx->P, S, ctx->keys, ctx->idx, ctx->stream);
+    return sort_perm(ctx, S.n);
+}
+
 int emu_ctx::resort_now(emu_context* ctx, unsigned* perm)
 {
     int r;

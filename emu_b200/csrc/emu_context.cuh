@@ -98,6 +98,10 @@ int record_stats(emu_context* ctx, int64_t n, double& pupt_min, double tot[2], d
 // re-sort the particles by cell now; when perm is not null it receives the
 // gather permutation (new slot i holds old slot perm[i])
 int resort_now(emu_context* ctx, unsigned* perm);
+// the cell-sort gather permutation of the particles of S (positions, count
+// and capacity of S; the context's sort buffers): ctx->idx2, new slot i
+// holds slot idx2[i]
+int sort_state_perm(emu_context* ctx, const DevState& S);
 // frees the adjoint arrays (emu_destroy)
 void adjoint_free(emu_context* ctx);
 
