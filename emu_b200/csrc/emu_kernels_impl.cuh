@@ -778,12 +778,24 @@ __device__ __forceinline__ void potential_fp64_sp(const DevParams& P, const doub
         const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
         const double* __restrict__ m = mesh + cell * ND;
         const double coef = ((P.sqrt2GF_inv_vol * st.wx[ii]) * st.wy[jj]) * st.wz[kk];
+        // the cell's 8 NH values (two flavors: 16-byte vector loads, every
+        // group of NH = 4 starts on a 32-byte boundary)
+        double c[ND];
+        if constexpr (NH % 2 == 0) {
+#pragma unroll
+            for (int k = 0; k < ND / 2; k++) {
+                const double2 v = __ldg(reinterpret_cast<const double2*>(m) + k);
+                c[2 * k] = v.x;
+                c[2 * k + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < ND; k++) c[k] = __ldg(m + k);
+        }
 #pragma unroll
         for (int e = 0; e < NH; e++) {
-            const double SI = __ldg(m + e) - __ldg(m + 2 * NH + e) * vx - __ldg(m + 4 * NH + e) * vy -
-                              __ldg(m + 6 * NH + e) * vz;
-            const double Sb = __ldg(m + NH + e) - __ldg(m + 3 * NH + e) * vx - __ldg(m + 5 * NH + e) * vy -
-                              __ldg(m + 7 * NH + e) * vz;
+            const double SI = c[e] - c[2 * NH + e] * vx - c[4 * NH + e] * vy - c[6 * NH + e] * vz;
+            const double Sb = c[NH + e] - c[3 * NH + e] * vx - c[5 * NH + e] * vy - c[7 * NH + e] * vz;
             double inside = H::is_im(e) ? SI + Sb : SI - Sb;
             if (e == 0) inside = inside + P.matter;
             const double t = coef * inside;
