@@ -918,9 +918,9 @@ void free_adj(emu_adjoint* a)
     for (void* p : {(void*)a->dts_dev, (void*)a->ck, (void*)a->seg, (void*)a->work, (void*)a->nex, (void*)a->rows,
                     (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst, (void*)a->map[0], (void*)a->map[1],
                     (void*)a->wf2, (void*)a->wpos2, (void*)a->gperm, (void*)a->smap})
-        if (p) cudaFree(p);
+        if (p) emu_ctx::dev_free(p);
     for (int i = 0; i < 4; i++)
-        if (a->lmesh[i]) cudaFree(a->lmesh[i]);
+        if (a->lmesh[i]) emu_ctx::dev_free(a->lmesh[i]);
     delete a;
 }
 
@@ -1004,7 +1004,7 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         a->bytes = 0;
         auto alloc = [&](auto** ptr, size_t b) {
             a->bytes += b;
-            return cudaMalloc(reinterpret_cast<void**>(ptr), b);
+            return emu_ctx::dev_malloc(reinterpret_cast<void**>(ptr), b);
         };
         CU(alloc(&a->dts_dev, sizeof(double) * a->dts.size()));
         CU(alloc(&a->ck, sizeof(double) * slot * a->ck_slots));

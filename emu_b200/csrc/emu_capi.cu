@@ -21,6 +21,12 @@ int widths(int ord) { return ord >= 2 ? 3 : (ord == 1 ? 2 : 1); }
 
 }  // namespace
 
+std::recursive_mutex& emu_ctx::device_lock()
+{
+    static std::recursive_mutex m;
+    return m;
+}
+
 int emu_ctx::fail(emu_context* c, int code, const std::string& msg)
 {
     if (c) c->err = msg; else g_host_err = msg;
@@ -155,11 +161,12 @@ int ensure_capacity(emu_context* ctx, long long n)
     if (n <= ctx->cap && ctx->pblock[0]) return EMU_OK;
     free_graphs(ctx);
     for (int i = 0; i < 2; i++)
-        if (ctx->pblock[i]) cudaFree(ctx->pblock[i]);
-    if (ctx->tblock) cudaFree(ctx->tblock);
-    if (ctx->S[0].kgen) cudaFree(ctx->S[0].kgen);
-    if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
-    if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
+        if (ctx->pblock[i]) emu_ctx::dev_free(ctx->pblock[i]);
+    if (ctx->tblock) emu_ctx::dev_free(ctx->tblock);
+    if (ctx->S[0].kgen) emu_ctx::dev_free(ctx->S[0].kgen);
+    for (void* a : {(void*)ctx->keys, (void*)ctx->keys2, (void*)ctx->idx, (void*)ctx->idx2})
+        if (a) emu_ctx::dev_free(a);
+    if (ctx->sort_tmp) emu_ctx::dev_free(ctx->sort_tmp);
     ctx->pblock[0] = ctx->pblock[1] = ctx->tblock = nullptr;
     ctx->keys = ctx->keys2 = ctx->idx = ctx->idx2 = nullptr;
     ctx->sort_tmp = nullptr;
@@ -168,20 +175,20 @@ int ensure_capacity(emu_context* ctx, long long n)
     // 16-byte aligned block that bulk copies may read in full
     const long long cap = (std::max<long long>(n, 1) + 127) / 128 * 128;
     for (int i = 0; i < 2; i++) {
-        CU(cudaMalloc(&ctx->pblock[i], persistent_bytes(ctx->NS, ctx->mixed, cap)));
+        CU(emu_ctx::dev_malloc(&ctx->pblock[i], persistent_bytes(ctx->NS, ctx->mixed, cap)));
         ctx->S[i] = DevState();
         assign_persistent(ctx->S[i], ctx->pblock[i], ctx->NS, ctx->mixed, cap);
     }
-    CU(cudaMalloc(&ctx->tblock, transient_bytes(ctx->NS, ctx->mixed, cap)));
+    CU(emu_ctx::dev_malloc(&ctx->tblock, transient_bytes(ctx->NS, ctx->mixed, cap)));
     for (int i = 0; i < 2; i++) assign_transient(ctx->S[i], ctx->tblock, ctx->NS, ctx->mixed, cap);
-    CU(cudaMalloc(&ctx->keys, sizeof(unsigned) * cap));
-    CU(cudaMalloc(&ctx->keys2, sizeof(unsigned) * cap));
-    CU(cudaMalloc(&ctx->idx, sizeof(unsigned) * cap));
-    CU(cudaMalloc(&ctx->idx2, sizeof(unsigned) * cap));
+    CU(emu_ctx::dev_malloc(&ctx->keys, sizeof(unsigned) * cap));
+    CU(emu_ctx::dev_malloc(&ctx->keys2, sizeof(unsigned) * cap));
+    CU(emu_ctx::dev_malloc(&ctx->idx, sizeof(unsigned) * cap));
+    CU(emu_ctx::dev_malloc(&ctx->idx2, sizeof(unsigned) * cap));
     size_t tb = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tb, ctx->keys, ctx->keys2, ctx->idx, ctx->idx2, (int)cap);
     ctx->sort_tmp_bytes = tb + 256;
-    CU(cudaMalloc(&ctx->sort_tmp, ctx->sort_tmp_bytes));
+    CU(emu_ctx::dev_malloc(&ctx->sort_tmp, ctx->sort_tmp_bytes));
     ctx->cap = cap;
     return EMU_OK;
 }
@@ -189,9 +196,9 @@ int ensure_capacity(emu_context* ctx, long long n)
 int ensure_aos(emu_context* ctx, long long n)
 {
     if (n <= ctx->aos_cap && ctx->aos) return EMU_OK;
-    if (ctx->aos) cudaFree(ctx->aos);
+    if (ctx->aos) emu_ctx::dev_free(ctx->aos);
     ctx->aos = nullptr;
-    CU(cudaMalloc(&ctx->aos, sizeof(double) * (size_t)std::max<long long>(n, 1) * ctx->nreal));
+    CU(emu_ctx::dev_malloc(&ctx->aos, sizeof(double) * (size_t)std::max<long long>(n, 1) * ctx->nreal));
     ctx->aos_cap = std::max<long long>(n, 1);
     return EMU_OK;
 }
@@ -353,7 +360,7 @@ int step_generic(emu_context* ctx, double dt)
     DevState& S = ctx->S[ctx->cur];
     const long long kstride = (long long)ctx->NS * ctx->cap;
     if (!S.kgen) {
-        CU(cudaMalloc(&ctx->S[0].kgen, sizeof(double) * 4 * kstride));
+        CU(emu_ctx::dev_malloc(&ctx->S[0].kgen, sizeof(double) * 4 * kstride));
         ctx->S[1].kgen = ctx->S[0].kgen;
     }
     int r;
@@ -416,9 +423,14 @@ int enqueue_step_body(emu_context* ctx, cudaStream_t st, bool dep4)
 int build_graph(emu_context* ctx, int variant)
 {
     cudaGraph_t g = nullptr;
-    CU(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
-    int r = enqueue_step_body(ctx, ctx->cap_stream, variant == 0);
-    cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &g);
+    int r;
+    cudaError_t e;
+    {
+        std::lock_guard<std::recursive_mutex> lock(emu_ctx::device_lock());
+        CU(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal));
+        r = enqueue_step_body(ctx, ctx->cap_stream, variant == 0);
+        e = cudaStreamEndCapture(ctx->cap_stream, &g);
+    }
     if (r) {
         if (g) cudaGraphDestroy(g);
         return r;
@@ -599,30 +611,33 @@ int emu_create(const emu_params* p, emu_context** out)
     const size_t me = (size_t)mesh_elems(ctx);
     if (ctx->mixed) {
         for (int i = 0; i < 2 && !r; i++)
-            if (cudaMalloc(&ctx->qmesh[i], sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
-        if (!r && cudaMalloc(&ctx->qfull, sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
-        if (!r && cudaMalloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * 4 * ctx->NH) != cudaSuccess)
+            if (emu_ctx::dev_malloc(&ctx->qmesh[i], sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+        if (!r && emu_ctx::dev_malloc(&ctx->qfull, sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+        if (!r && emu_ctx::dev_malloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * 4 * ctx->NH) != cudaSuccess)
             r = EMU_ERR_NOMEM;
     } else {
         for (int i = 0; i < 4 && !r; i++)
-            if (cudaMalloc(&ctx->mesh[i], sizeof(double) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+            if (emu_ctx::dev_malloc(&ctx->mesh[i], sizeof(double) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
     }
-    if (!r && cudaMalloc(&ctx->planes, sizeof(double) * ctx->P.ncells * emu_ncomp(ctx->nf)) != cudaSuccess)
+    if (!r && emu_ctx::dev_malloc(&ctx->planes, sizeof(double) * ctx->P.ncells * emu_ncomp(ctx->nf)) != cudaSuccess)
         r = EMU_ERR_NOMEM;
-    if (!r && cudaMalloc(&ctx->ctl, sizeof(StepCtl)) != cudaSuccess) r = EMU_ERR_NOMEM;
-    if (!r && cudaMallocHost(&ctx->ctl_host, sizeof(StepCtl)) != cudaSuccess) r = EMU_ERR_NOMEM;
+    if (!r && emu_ctx::dev_malloc(&ctx->ctl, sizeof(StepCtl)) != cudaSuccess) r = EMU_ERR_NOMEM;
+    if (!r && emu_ctx::host_malloc(&ctx->ctl_host, sizeof(StepCtl)) != cudaSuccess) r = EMU_ERR_NOMEM;
     if (r) {
         ctx->err = "emu_create: device allocation failed";
         return bail(r);
     }
-    cudaMemset(ctx->ctl, 0, sizeof(StepCtl));
+    // on the context's own stream: a device-wide synchronisation would
+    // break another thread's graph capture
     std::memset(ctx->ctl_host, 0, sizeof(StepCtl));
+    e = cudaMemsetAsync(ctx->ctl, 0, sizeof(StepCtl), ctx->own);
     for (int i = 0; i < 4; i++)
-        if (ctx->mesh[i]) cudaMemset(ctx->mesh[i], 0, sizeof(double) * me);
+        if (ctx->mesh[i] && e == cudaSuccess) e = cudaMemsetAsync(ctx->mesh[i], 0, sizeof(double) * me, ctx->own);
     for (int i = 0; i < 2; i++)
-        if (ctx->qmesh[i]) cudaMemset(ctx->qmesh[i], 0, sizeof(long long) * me);
-    if (ctx->qfull) cudaMemset(ctx->qfull, 0, sizeof(long long) * me);
-    if (cudaDeviceSynchronize() != cudaSuccess) {
+        if (ctx->qmesh[i] && e == cudaSuccess) e = cudaMemsetAsync(ctx->qmesh[i], 0, sizeof(long long) * me, ctx->own);
+    if (ctx->qfull && e == cudaSuccess) e = cudaMemsetAsync(ctx->qfull, 0, sizeof(long long) * me, ctx->own);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->own);
+    if (e != cudaSuccess) {
         ctx->err = "emu_create: device initialisation failed";
         return bail(EMU_ERR_CUDA);
     }
@@ -635,22 +650,23 @@ void emu_destroy(emu_context* ctx)
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_graphs(ctx);
-    for (int i = 0; i < 2; i++) if (ctx->pblock[i]) cudaFree(ctx->pblock[i]);
-    if (ctx->tblock) cudaFree(ctx->tblock);
-    if (ctx->S[0].kgen) cudaFree(ctx->S[0].kgen);
-    for (int i = 0; i < 4; i++) if (ctx->mesh[i]) cudaFree(ctx->mesh[i]);
-    for (int i = 0; i < 2; i++) if (ctx->qmesh[i]) cudaFree(ctx->qmesh[i]);
-    if (ctx->qfull) cudaFree(ctx->qfull);
-    if (ctx->gmesh) cudaFree(ctx->gmesh);
-    if (ctx->fmesh_tmp) cudaFree(ctx->fmesh_tmp);
-    if (ctx->planes) cudaFree(ctx->planes);
-    if (ctx->ctl) cudaFree(ctx->ctl);
-    if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
-    if (ctx->aos) cudaFree(ctx->aos);
-    if (ctx->keys) { cudaFree(ctx->keys); cudaFree(ctx->keys2); cudaFree(ctx->idx); cudaFree(ctx->idx2); }
-    if (ctx->sort_tmp) cudaFree(ctx->sort_tmp);
-    if (ctx->stats) cudaFree(ctx->stats);
-    if (ctx->stats_host) cudaFreeHost(ctx->stats_host);
+    for (int i = 0; i < 2; i++) if (ctx->pblock[i]) emu_ctx::dev_free(ctx->pblock[i]);
+    if (ctx->tblock) emu_ctx::dev_free(ctx->tblock);
+    if (ctx->S[0].kgen) emu_ctx::dev_free(ctx->S[0].kgen);
+    for (int i = 0; i < 4; i++) if (ctx->mesh[i]) emu_ctx::dev_free(ctx->mesh[i]);
+    for (int i = 0; i < 2; i++) if (ctx->qmesh[i]) emu_ctx::dev_free(ctx->qmesh[i]);
+    if (ctx->qfull) emu_ctx::dev_free(ctx->qfull);
+    if (ctx->gmesh) emu_ctx::dev_free(ctx->gmesh);
+    if (ctx->fmesh_tmp) emu_ctx::dev_free(ctx->fmesh_tmp);
+    if (ctx->planes) emu_ctx::dev_free(ctx->planes);
+    if (ctx->ctl) emu_ctx::dev_free(ctx->ctl);
+    if (ctx->ctl_host) emu_ctx::host_free(ctx->ctl_host);
+    if (ctx->aos) emu_ctx::dev_free(ctx->aos);
+    for (void* a : {(void*)ctx->keys, (void*)ctx->keys2, (void*)ctx->idx, (void*)ctx->idx2})
+        if (a) emu_ctx::dev_free(a);
+    if (ctx->sort_tmp) emu_ctx::dev_free(ctx->sort_tmp);
+    if (ctx->stats) emu_ctx::dev_free(ctx->stats);
+    if (ctx->stats_host) emu_ctx::host_free(ctx->stats_host);
     emu_ctx::adjoint_free(ctx);
     emu_ctx_comm_free(ctx);
     if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -757,13 +773,13 @@ int emu_interpolate_rhs(emu_context* ctx, double* rhs_records)
     DevState& S = ctx->S[ctx->cur];
     const long long kstride = (long long)ctx->NS * ctx->cap;
     if (!S.kgen) {
-        CU(cudaMalloc(&ctx->S[0].kgen, sizeof(double) * 4 * kstride));
+        CU(emu_ctx::dev_malloc(&ctx->S[0].kgen, sizeof(double) * 4 * kstride));
         ctx->S[1].kgen = ctx->S[0].kgen;
     }
     const double* mesh = nullptr;
     if (ctx->mixed) {
         // the FP64 interpolation of the fixed-point mesh
-        if (!ctx->fmesh_tmp) CU(cudaMalloc(&ctx->fmesh_tmp, sizeof(double) * mesh_elems(ctx)));
+        if (!ctx->fmesh_tmp) CU(emu_ctx::dev_malloc(&ctx->fmesh_tmp, sizeof(double) * mesh_elems(ctx)));
         emu::launch_q_to_f64(ctx->nf, ctx->P, q_current(ctx), ctx->fmesh_tmp, ctx->stream);
         mesh = ctx->fmesh_tmp;
     } else {

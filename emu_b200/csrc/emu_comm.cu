@@ -91,7 +91,7 @@ void emu_ctx_comm_free(emu_context* ctx)
 {
     if (ctx->comm) nccl().CommDestroy(static_cast<ncclComm_t>(ctx->comm));
     ctx->comm = nullptr;
-    if (ctx->red_scratch) cudaFree(ctx->red_scratch);
+    if (ctx->red_scratch) emu_ctx::dev_free(ctx->red_scratch);
     ctx->red_scratch = nullptr;
 }
 
@@ -126,7 +126,7 @@ int emu_attach_comm(emu_context* ctx, const char* id, int rank, int nranks)
     ctx->comm = c;
     ctx->rank = rank;
     ctx->nranks = nranks;
-    CU(cudaMalloc(&ctx->red_scratch, 8 * sizeof(double)));
+    CU(emu_ctx::dev_malloc(&ctx->red_scratch, 8 * sizeof(double)));
     return EMU_OK;
 }
 

@@ -6,6 +6,7 @@
 #include "emu_host.h"
 #include "emu_kernels.cuh"
 
+#include <mutex>
 #include <string>
 
 using emu::DevParams;
@@ -66,6 +67,35 @@ struct emu_context {
 };
 
 namespace emu_ctx {
+
+// Device-wide CUDA calls (allocation and release of device and pinned
+// memory) fail while another thread's stream is being captured into a graph,
+// and invalidate that capture. Contexts may be driven from several host
+// threads at once, so these calls and the graph captures hold one
+// process-wide (recursive) lock.
+std::recursive_mutex& device_lock();
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes)
+{
+    std::lock_guard<std::recursive_mutex> g(device_lock());
+    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+template <class T>
+cudaError_t host_malloc(T** p, size_t bytes)
+{
+    std::lock_guard<std::recursive_mutex> g(device_lock());
+    return cudaMallocHost(reinterpret_cast<void**>(p), bytes);
+}
+inline cudaError_t dev_free(void* p)
+{
+    std::lock_guard<std::recursive_mutex> g(device_lock());
+    return cudaFree(p);
+}
+inline cudaError_t host_free(void* p)
+{
+    std::lock_guard<std::recursive_mutex> g(device_lock());
+    return cudaFreeHost(p);
+}
 
 // record msg on the context (or the thread's host error when c is null)
 int fail(emu_context* c, int code, const std::string& msg);

@@ -71,8 +71,8 @@ constexpr int kStatBlocks = 1184;
 int emu_ctx::record_stats(emu_context* ctx, int64_t n, double& pupt_min, double tot[2], double mx[2])
 {
     if (!ctx->stats) {
-        CU(cudaMalloc(&ctx->stats, sizeof(double) * 5 * kStatBlocks));
-        CU(cudaMallocHost(&ctx->stats_host, sizeof(double) * 5 * kStatBlocks));
+        CU(emu_ctx::dev_malloc(&ctx->stats, sizeof(double) * 5 * kStatBlocks));
+        CU(emu_ctx::host_malloc(&ctx->stats_host, sizeof(double) * 5 * kStatBlocks));
     }
     const int nblk = (int)std::max<long long>(1, std::min<long long>((n + kStatBlock - 1) / kStatBlock, kStatBlocks));
     k_record_stats<<<nblk, kStatBlock, 0, ctx->stream>>>(ctx->aos, n, ctx->nreal, ctx->NH, ctx->stats);
@@ -108,10 +108,10 @@ extern "C" int emu_init_particles_device(emu_context* ctx)
     double* ddirs = nullptr;
     int* bad = nullptr;
     auto release = [&]() {
-        if (ddirs) cudaFree(ddirs);
-        if (bad) cudaFree(bad);
+        if (ddirs) emu_ctx::dev_free(ddirs);
+        if (bad) emu_ctx::dev_free(bad);
     };
-    if (cudaMalloc(&ddirs, sizeof(double) * dirs.size()) != cudaSuccess || cudaMalloc(&bad, sizeof(int)) != cudaSuccess) {
+    if (emu_ctx::dev_malloc(&ddirs, sizeof(double) * dirs.size()) != cudaSuccess || emu_ctx::dev_malloc(&bad, sizeof(int)) != cudaSuccess) {
         release();
         return fail(ctx, EMU_ERR_NOMEM, "emu_init_particles_device: scratch allocation failed");
     }
