@@ -1260,7 +1260,7 @@ constexpr int mixed_stage_smem_bytes()
     constexpr int tile = tile_smem_bytes<NF, SW<WX, WY, WZ>, float>();
     using SWt = SW<WX, WY, WZ>;
     constexpr bool preload = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
-    constexpr int staged = preload ? 0 : 2 * NF * NF * kBlock * 16;
+    constexpr int staged = preload ? 0 : 2 * NF * NF * kBlock * 16 + 7 * kBlock * 8;
     return tile > staged ? tile : staged;
 }
 
@@ -1294,6 +1294,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     double* const sf0 = reinterpret_cast<double*>(tile_smem);        // [NS][kBlock]
     float* const sk = reinterpret_cast<float*>(sf0 + NS * kBlock);   // [NS][kBlock]
     float* const sks = sk + NS * kBlock;                             // [NS][kBlock]
+    double* const s4 = reinterpret_cast<double*>(sks + NS * kBlock); // stage 4: time, pup[4], L[2] x kBlock
     const long long p0 = (long long)blockIdx.x * kBlock;
     if constexpr (STAGE) {
         // f0 is written only by the previous step: its copies start before
@@ -1301,10 +1302,17 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         if (t < 32) {
             if (t == 0) {
                 mbar_init(&stage_bar, 1);
-                mbar_expect_tx(&stage_bar, NS * kBlock * 8 + (s > 1 ? 2 * NS * kBlock * 4 : 0));
+                mbar_expect_tx(&stage_bar, NS * kBlock * 8 + (s > 1 ? 2 * NS * kBlock * 4 : 0) +
+                                               (s == 4 ? 7 * kBlock * 8 : 0));
             }
             __syncwarp();
             for (int c = t; c < NS; c += 32) bulk_g2s(sf0 + c * kBlock, S.f0 + c * cap + p0, kBlock * 8, &stage_bar);
+            // stage 4's time, momentum and SU(n) lengths (written only by
+            // the previous step too)
+            if (s == 4 && t < 7) {
+                const double* src = t == 0 ? S.time : t < 5 ? S.pup[t - 1] : S.Ll[t - 5];
+                bulk_g2s(s4 + t * kBlock, src + p0, kBlock * 8, &stage_bar);
+            }
         }
         __syncthreads();   // the barrier is initialised before anyone waits on it
     }
@@ -1438,7 +1446,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     else ks = sks[(sp * NH + e) * kBlock + t];
                     fn[e] = y0[e] + w6 * ((double)ks + (Kv[e] + (double)ksi[e]));
                 }
-                stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : S.Ll[sp][p], P.maxError);
+                stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : s4[(5 + sp) * kBlock + t], P.maxError);
 #pragma unroll
                 for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
             }
@@ -1448,9 +1456,9 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         }
         if (s == 4) {
             double xn[3] = {x, y, z};
-            double tn = PRELOAD ? t_in : S.time[p];
-            const double pq[4] = {PRELOAD ? pu[0] : S.pup[0][p], PRELOAD ? pu[1] : S.pup[1][p],
-                                  PRELOAD ? pu[2] : S.pup[2][p], PRELOAD ? pu[3] : S.pup[3][p]};
+            double tn = PRELOAD ? t_in : s4[t];
+            const double pq[4] = {PRELOAD ? pu[0] : s4[kBlock + t], PRELOAD ? pu[1] : s4[2 * kBlock + t],
+                                  PRELOAD ? pu[2] : s4[3 * kBlock + t], PRELOAD ? pu[3] : s4[4 * kBlock + t]};
             const double ipt = 1.0 / pq[3];
             const double kxv[3] = {pq[0] * ipt * kC, pq[1] * ipt * kC, pq[2] * ipt * kC};
 #pragma unroll
