@@ -149,7 +149,10 @@ int emu_init_particles_device(emu_context* ctx);
 int emu_vvac_max(const emu_params* p, const double* records, int64_t n, double* out);
 
 /* ---- context (needs a CUDA device) ---- */
-/* Creates the device context; the caller owns it. */
+/* Creates the device context; the caller owns it.  Different contexts may be
+ * driven from different host threads at once (one thread per context); the
+ * library serialises its allocations and graph captures internally and makes
+ * no device-wide synchronisation.  One context is not thread safe. */
 int emu_create(const emu_params* p, emu_context** out);
 void emu_destroy(emu_context* ctx);
 /* Launch all work of this context on a caller-provided cudaStream_t (NULL =
