@@ -84,6 +84,10 @@ struct emu_adjoint {
     unsigned* gperm = nullptr;
     unsigned* smap = nullptr;
     int gslots = 0, sslots = 0;
+    // and, when the free memory allows, the meshes M_1..M_4 of every step of
+    // a sub-segment (gslots x 4 x nmesh) as the state pass deposits them: the
+    // sweep's stage recompute then only interpolates
+    double* smesh = nullptr;
 };
 
 namespace emu {
@@ -256,7 +260,7 @@ __device__ __forceinline__ void adj_fwd_stage_body(const DevParams& P, const Dev
             }
         }
     }
-    if (s < 4)
+    if (s < 4 && mesh_out)   // (null: the stage meshes are stored)
         tile_deposit_block<NF, SWt, double>(P, mesh_out, active, st, fN, vx, vy, vz,
                                             [](double a, int) -> double { return a; });
 }
@@ -917,7 +921,7 @@ void free_adj(emu_adjoint* a)
     if (!a) return;
     for (void* p : {(void*)a->dts_dev, (void*)a->ck, (void*)a->seg, (void*)a->work, (void*)a->nex, (void*)a->rows,
                     (void*)a->perm, (void*)a->stat, (void*)a->sst, (void*)a->mst, (void*)a->map[0], (void*)a->map[1],
-                    (void*)a->wf2, (void*)a->wpos2, (void*)a->gperm, (void*)a->smap})
+                    (void*)a->wf2, (void*)a->wpos2, (void*)a->gperm, (void*)a->smap, (void*)a->smesh})
         if (p) emu_ctx::dev_free(p);
     for (int i = 0; i < 4; i++)
         if (a->lmesh[i]) emu_ctx::dev_free(a->lmesh[i]);
@@ -1027,6 +1031,11 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
             CU(alloc(&a->wpos2, sizeof(double) * (size_t)3 * cap));
             CU(alloc(&a->gperm, sizeof(unsigned) * (size_t)a->gslots * cap));
             CU(alloc(&a->smap, sizeof(unsigned) * (size_t)a->sslots * cap));
+            size_t f2 = 0, t2 = 0;
+            cudaMemGetInfo(&f2, &t2);
+            const size_t mb = sizeof(double) * (size_t)a->gslots * 4 * nm;
+            const char* menv = std::getenv("EMU_ADJOINT_STORE_MESHES");
+            if ((!menv || std::atoi(menv) != 0) && mb + ((size_t)2 << 30) <= f2) CU(alloc(&a->smesh, mb));
         }
         double* w = a->work;
         a->acc = w; w += (size_t)NS * cap;
@@ -1079,14 +1088,18 @@ int deposit_into(emu_context* ctx, const DevState& S, const double* f, double* m
 }
 
 // forward over steps [0, len) of G (step 0's Y_0, x in place, stored meshes
-// zeroed), storing stage states and meshes, then the backward sweep
-int segment_sweep(emu_context* ctx, const DevState& W, const emu::SegPtrs& G, bool coop)
+// zeroed), storing stage states and meshes, then the backward sweep.
+// meshes_given: G's meshes M_1..M_4 already hold the step's deposits (one
+// step, not cooperative); the forward only recomputes the stage states.
+int segment_sweep(emu_context* ctx, const DevState& W, const emu::SegPtrs& G, bool coop, bool meshes_given = false)
 {
     const int nf = ctx->nf;
     const long long cap = ctx->cap;
     cudaStream_t st = ctx->stream;
     int r;
-    if ((r = deposit_into(ctx, emu::seg_state(W, G, 0), emu::seg_f(G, 0), emu::seg_m(G, 0, 0)))) return r;
+    if (!meshes_given &&
+        (r = deposit_into(ctx, emu::seg_state(W, G, 0), emu::seg_f(G, 0), emu::seg_m(G, 0, 0))))
+        return r;
     if (coop) {
         cudaError_t e = emu::launch_adj_seg_coop(nf, true, ctx->P, W, G, ctx->ctl, st);
         if (e == cudaSuccess) e = emu::launch_adj_seg_coop(nf, false, ctx->P, W, G, ctx->ctl, st);
@@ -1099,7 +1112,8 @@ int segment_sweep(emu_context* ctx, const DevState& W, const emu::SegPtrs& G, bo
         const double* Y0 = emu::seg_f(G, j);
         for (int s = 1; s <= 3; s++)
             emu::launch_adj_fwd_stage(nf, ctx->P, Q, s, dt, s == 1 ? Y0 : emu::seg_y(G, j, s, cap), Y0, G.acc,
-                                      emu::seg_y(G, j, s + 1, cap), emu::seg_m(G, j, s - 1), emu::seg_m(G, j, s), st);
+                                      emu::seg_y(G, j, s + 1, cap), emu::seg_m(G, j, s - 1),
+                                      meshes_given ? nullptr : emu::seg_m(G, j, s), st);
         const bool more = j + 1 < G.len;
         emu::launch_adj_fwd_stage4_next(nf, ctx->P, Q, dt, emu::seg_y(G, j, 4, cap), G.acc, emu::seg_y(G, j, 5, cap),
                                         more ? emu::seg_f(G, j + 1) : nullptr,
@@ -1442,18 +1456,26 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
                 res = 1;
                 return EMU_OK;
             };
-            auto restore = [&](const double* slot) -> int {
+            // the recompute state from a slot, its deposit into m1 and m2
+            // zeroed (stage 1 deposits there)
+            auto restore = [&](const double* slot, double* m1, double* m2) -> int {
                 CU(cudaMemcpyAsync(rf, slot, sizeof(double) * NS * cap, cudaMemcpyDeviceToDevice, st));
                 CU(cudaMemcpyAsync(rp, slot + (size_t)NS * cap, sizeof(double) * 3 * cap, cudaMemcpyDeviceToDevice,
                                    st));
-                CU(cudaMemsetAsync(M[1], 0, sizeof(double) * nm, st));
-                return deposit_into(ctx, Rv(), rf, M[0]);
+                CU(cudaMemsetAsync(m2, 0, sizeof(double) * nm, st));
+                return deposit_into(ctx, Rv(), rf, m1);
             };
-            auto advance = [&]() {
+            // one step: stage s reads q[s-1], deposits into q[s] and zeroes
+            // q[s+1] (q[4], q[5]: M_1 and M_2 of the next step)
+            auto advance_q = [&](double* const q[6]) {
                 const DevState R = Rv();
                 for (int s = 1; s <= 4; s++)
-                    emu::launch_rk4_stage(nf, ctx->P, R, s, M[s - 1], M[s % 4], M[(s + 1) % 4], nm, ctx->ctl, -1, st);
+                    emu::launch_rk4_stage(nf, ctx->P, R, s, q[s - 1], q[s], q[s + 1], nm, ctx->ctl, -1, st);
             };
+            double* const Mr[6] = {M[0], M[1], M[2], M[3], M[0], M[1]};   // the context's rotating meshes
+            auto advance = [&]() { advance_q(Mr); };
+            // stored meshes of sub-segment step j (M_1..M_4 at q = 0..3)
+            auto Mk = [&](int j, int q) -> double* { return a->smesh + ((size_t)j * 4 + q) * nm; };
             const bool mapped = seg + 1 < a->nck ? a->resorted[seg + 1] != 0 : a->final_mapped;
             if (mapped && (r = move_static(a->perm + (size_t)(seg + 1) * cap, true, false))) return r;
             // sub-checkpoints (seg slot J + i) and the composed map of every
@@ -1461,7 +1483,7 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
             // i + 1 -> slot at sub-checkpoint i)
             std::vector<int> ncomp(nsub, 0);
             if (nsub > 1) {
-                if ((r = restore(slot_f(a, a->ck, seg)))) return r;
+                if ((r = restore(slot_f(a, a->ck, seg), M[0], M[1]))) return r;
                 const int kl = k0 + (nsub - 1) * J;
                 int mc = 0;
                 for (int k = k0; k <= kl; k++) {
@@ -1487,27 +1509,46 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
             for (int i = nsub - 1; i >= 0; i--) {
                 const int s0 = k0 + i * J, s1 = std::min(s0 + J, k1);
                 if (i < nsub - 1 && ncomp[i] && (r = move_static(a->smap + (size_t)i * cap, true, false))) return r;
-                if ((r = restore(i == 0 ? slot_f(a, a->ck, seg) : slot_f(a, a->seg, J + i)))) return r;
-                std::vector<int> has(s1 - s0, 0);
+                const double* slot0 = i == 0 ? slot_f(a, a->ck, seg) : slot_f(a, a->seg, J + i);
+                const bool keep = a->smesh != nullptr;
+                if ((r = keep ? restore(slot0, Mk(0, 0), Mk(0, 1)) : restore(slot0, M[0], M[1]))) return r;
+                std::vector<int> has(s1 - s0, 0), meshed(s1 - s0, 0);
                 for (int k = s0; k < s1; k++) {
-                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(Rv(), slot_f(a, a->seg, k - s0), NS, a->dts_dev, k,
+                    const int j = k - s0;
+                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(Rv(), slot_f(a, a->seg, j), NS, a->dts_dev, k,
                                                                 ctx->ctl);
                     const bool due = k + 1 < a->nsteps && (k + 1) % ri == 0;
                     if (k + 1 < s1 || due) {
                         // (the last step too when a re-sort follows it: its
                         // permutation maps onto the next sub-segment's order)
-                        advance();
-                        if ((r = resort_after(k, a->gperm + (size_t)(k - s0) * cap, has[k - s0]))) return r;
+                        if (keep) {
+                            const bool nx = k + 1 < s1;
+                            double* const q[6] = {Mk(j, 0), Mk(j, 1), Mk(j, 2),
+                                                  Mk(j, 3), nx ? Mk(j + 1, 0) : M[0], nx ? Mk(j + 1, 1) : M[1]};
+                            advance_q(q);
+                            meshed[j] = 1;
+                        } else {
+                            advance();
+                        }
+                        if ((r = resort_after(k, a->gperm + (size_t)j * cap, has[j]))) return r;
                     }
                 }
                 if ((r = check_launch(ctx, "adjoint segment recompute"))) return r;
                 for (int k = s1 - 1; k >= s0; k--) {
-                    if (has[k - s0] && (r = move_static(a->gperm + (size_t)(k - s0) * cap, true, true))) return r;
-                    G.seg = slot_f(a, a->seg, k - s0);
+                    const int j = k - s0;
+                    if (has[j] && (r = move_static(a->gperm + (size_t)j * cap, true, true))) return r;
+                    G.seg = slot_f(a, a->seg, j);
                     G.k0 = k;
                     G.len = 1;
-                    CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * 4 * nm, st));
-                    if ((r = segment_sweep(ctx, Wv(), G, false))) return r;
+                    if (meshed[j]) {
+                        G.mst = Mk(j, 0);
+                        r = segment_sweep(ctx, Wv(), G, false, true);
+                        G.mst = a->mst;
+                    } else {
+                        CU(cudaMemsetAsync(a->mst, 0, sizeof(double) * 4 * nm, st));
+                        r = segment_sweep(ctx, Wv(), G, false);
+                    }
+                    if (r) return r;
                 }
             }
         } else {

@@ -183,16 +183,20 @@ def test_adjoint_memory_modes_agree(monkeypatch, store):
     assert _rel(gN, Nr.grad.numpy()) < 1e-9
 
 
-@pytest.mark.parametrize("store", ["segment", "per_step", "per_step_sub2"])
+@pytest.mark.parametrize("store", ["segment", "per_step", "per_step_sub2", "per_step_sub2_nomesh"])
 def test_adjoint_3d_resorted_every_step(monkeypatch, store):
     """3 flavors, 3D TSC: particles re-sorted after every step (the automatic
     interval).  The recorded forward composes a segment's re-sorts into one
     map; the per-step modes re-sort their recomputes too and undo each step's
-    permutation in the sweep.  Gradient against torch autograd."""
+    permutation in the sweep, with the stage meshes kept from the state pass
+    (or, nomesh, redeposited by the sweep's recompute).  Gradient against
+    torch autograd."""
     if store != "segment":
         monkeypatch.setenv("EMU_ADJOINT_STORE_MAX_BYTES", "0")
-    if store == "per_step_sub2":
+    if store.startswith("per_step_sub2"):
         monkeypatch.setenv("EMU_ADJOINT_SUBCHECKPOINT", "2")
+    if store.endswith("nomesh"):
+        monkeypatch.setenv("EMU_ADJOINT_STORE_MESHES", "0")
     p = W.c5_3d(n=3, ndirs=4, mixed=False)
     parts = api.init_particles(p)
     fc, nc = flavor_columns(3), number_columns(3)
