@@ -84,6 +84,7 @@ struct emu_adjoint {
     unsigned* gperm = nullptr;
     unsigned* smap = nullptr;
     int gslots = 0, sslots = 0;
+    int rps_slots = 0;          // segment slots the sub-segment layout uses
     // and, when the free memory allows, the meshes M_1..M_4 of every step of
     // a sub-segment (gslots x 4 x nmesh) as the state pass deposits them: the
     // sweep's stage recompute then only interpolates
@@ -947,6 +948,38 @@ DevState stat_view(emu_adjoint* a, int w, const DevState& like)
     return W;
 }
 
+// Sub-segments of a segment of len steps over B segment slots (per-step
+// mode with re-sorts).  Sub-segment i >= 1 starts from its sub-checkpoint in
+// slot i - 1 and keeps its later states in slots i, i + 1, ... (the
+// sub-checkpoints of the sub-segments after it are consumed by then);
+// sub-segment 0 starts from the segment checkpoint and keeps its later
+// states in slots 0, 1, ...  So sub-segment i holds at most B + 1 (i = 0) or
+// B - i + 1 steps.  The fewest sub-segments, the later ones as long as
+// allowed: the sub-checkpoint pass stops at the last one's start.  Returns
+// the starts relative to the segment (nsub + 1 entries, the last = len), or
+// nothing when B slots cannot hold len steps.
+std::vector<int> rps_layout(int len, int B)
+{
+    auto most = [&](int i) { return i == 0 ? B + 1 : B - i + 1; };
+    int nsub = 0;
+    long long tot = 0;
+    while (tot < len) {
+        if (most(nsub) <= 0) return {};
+        tot += most(nsub);
+        nsub++;
+    }
+    std::vector<int> L(nsub);
+    int rem = len;
+    for (int i = nsub - 1; i >= 1; i--) {
+        L[i] = std::min(most(i), rem - i);   // (at least one step left for each earlier one)
+        rem -= L[i];
+    }
+    L[0] = rem;
+    std::vector<int> sb(nsub + 1, 0);
+    for (int i = 0; i < nsub; i++) sb[i + 1] = sb[i] + L[i];
+    return sb;
+}
+
 // device arrays for a recorded run of nsteps with checkpoints every interval
 int ensure_adj(emu_context* ctx, int nsteps, int interval)
 {
@@ -1005,6 +1038,20 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
                 a->seg_slots = J + (interval + J - 1) / J;
             }
         }
+        // per-step mode with re-sorts: the sub-segment layout over the
+        // segment slots (EMU_ADJOINT_SEG_SLOTS: fewer slots, for tests)
+        std::vector<int> rps_sb;
+        if (!a->store && ctx->prm.resort_interval > 0) {
+            int B = a->seg_slots;
+            if (const char* env = std::getenv("EMU_ADJOINT_SEG_SLOTS")) B = std::max(1, std::min(B, std::atoi(env)));
+            rps_sb = rps_layout(interval, B);
+            if (rps_sb.empty()) {
+                free_adj(a);
+                ctx->adj = nullptr;
+                return fail(ctx, EMU_ERR_ARG, "adjoint: too few segment slots for the checkpoint interval");
+            }
+            a->rps_slots = B;
+        }
         a->bytes = 0;
         auto alloc = [&](auto** ptr, size_t b) {
             a->bytes += b;
@@ -1024,9 +1071,10 @@ int ensure_adj(emu_context* ctx, int nsteps, int interval)
         CU(alloc(&a->rows, sizeof(double) * (size_t)NS * cap));
         for (int i = 0; i < 2; i++) CU(alloc(&a->map[i], sizeof(unsigned) * cap));
         if (!a->store && ctx->prm.resort_interval > 0) {
-            const int J = a->sub > 0 ? a->sub : interval;
-            a->gslots = J;
-            a->sslots = (interval + J - 1) / J;
+            // (a shorter last segment may form one sub-segment of up to
+            // B + 1 steps; a full one has the most sub-segments)
+            a->gslots = std::min(a->rps_slots + 1, interval);
+            a->sslots = (int)rps_sb.size() - 1;
             CU(alloc(&a->wf2, sizeof(double) * (size_t)NS * cap));
             CU(alloc(&a->wpos2, sizeof(double) * (size_t)3 * cap));
             CU(alloc(&a->gperm, sizeof(unsigned) * (size_t)a->gslots * cap));
@@ -1409,8 +1457,19 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
             // before the step; W enters in the next segment's start order
             const int ri = ctx->prm.resort_interval;
             double* const* M = ctx->mesh;
-            const int J = (a->sub > 0 && a->sub < len) ? a->sub : len;   // steps per sub-segment
-            const int nsub = (len + J - 1) / J;
+            // sub-segment starts (absolute steps; sb[nsub] = k1), see rps_layout
+            std::vector<int> sb = rps_layout(len, a->rps_slots);
+            if (sb.empty()) return fail(ctx, EMU_ERR_STATE, "adjoint: sub-segment layout");
+            const int nsub = (int)sb.size() - 1;
+            for (int& b : sb) b += k0;
+            // the step state at step k of sub-segment i: its start is the
+            // segment checkpoint (i = 0) or the sub-checkpoint in slot i - 1;
+            // the later ones follow in slots (i = 0 ? 0 : i), ...
+            auto state_slot = [&](int i, int k) -> double* {
+                const int j = k - sb[i];
+                if (j == 0) return i == 0 ? slot_f(a, a->ck, seg) : slot_f(a, a->seg, i - 1);
+                return slot_f(a, a->seg, (i == 0 ? 0 : i) + j - 1);
+            };
             double *rf = a->wf, *rf2 = a->wf2, *rp = a->wpos, *rp2 = a->wpos2;
             auto Wv = [&]() {
                 DevState V = stat_view(a, w, S);
@@ -1478,21 +1537,22 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
             auto Mk = [&](int j, int q) -> double* { return a->smesh + ((size_t)j * 4 + q) * nm; };
             const bool mapped = seg + 1 < a->nck ? a->resorted[seg + 1] != 0 : a->final_mapped;
             if (mapped && (r = move_static(a->perm + (size_t)(seg + 1) * cap, true, false))) return r;
-            // sub-checkpoints (seg slot J + i) and the composed map of every
-            // sub-segment but the last (smap slot i: slot at sub-checkpoint
-            // i + 1 -> slot at sub-checkpoint i)
+            // sub-checkpoints (seg slot i - 1 for sub-segment i >= 1) and the
+            // composed map of every sub-segment but the last (smap slot i:
+            // slot at sub-checkpoint i + 1 -> slot at sub-checkpoint i)
             std::vector<int> ncomp(nsub, 0);
             if (nsub > 1) {
                 if ((r = restore(slot_f(a, a->ck, seg), M[0], M[1]))) return r;
-                const int kl = k0 + (nsub - 1) * J;
+                const int kl = sb[nsub - 1];
                 int mc = 0;
+                int i = 0;   // the sub-segment of step k
                 for (int k = k0; k <= kl; k++) {
-                    const bool save = k > k0 && (k - k0) % J == 0;
+                    while (k >= sb[i + 1]) i++;
+                    const bool save = i >= 1 && k == sb[i];
                     emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(
-                        Rv(), save ? slot_f(a, a->seg, J + (k - k0) / J) : nullptr, NS, a->dts_dev, k, ctx->ctl);
+                        Rv(), save ? slot_f(a, a->seg, i - 1) : nullptr, NS, a->dts_dev, k, ctx->ctl);
                     if (k == kl) break;
                     advance();
-                    const int i = (k - k0) / J;
                     int res;
                     if ((r = resort_after(k, nullptr, res))) return r;
                     if (res) {
@@ -1500,23 +1560,24 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
                         mc = 1 - mc;
                         ncomp[i]++;
                     }
-                    if ((k + 1 - k0) % J == 0 && ncomp[i])
+                    if (k + 1 == sb[i + 1] && ncomp[i])
                         CU(cudaMemcpyAsync(a->smap + (size_t)i * cap, a->map[mc], sizeof(unsigned) * n,
                                            cudaMemcpyDeviceToDevice, st));
                 }
                 if ((r = check_launch(ctx, "adjoint sub-checkpoints"))) return r;
             }
             for (int i = nsub - 1; i >= 0; i--) {
-                const int s0 = k0 + i * J, s1 = std::min(s0 + J, k1);
+                const int s0 = sb[i], s1 = sb[i + 1];
                 if (i < nsub - 1 && ncomp[i] && (r = move_static(a->smap + (size_t)i * cap, true, false))) return r;
-                const double* slot0 = i == 0 ? slot_f(a, a->ck, seg) : slot_f(a, a->seg, J + i);
+                const double* slot0 = state_slot(i, s0);
                 const bool keep = a->smesh != nullptr;
                 if ((r = keep ? restore(slot0, Mk(0, 0), Mk(0, 1)) : restore(slot0, M[0], M[1]))) return r;
                 std::vector<int> has(s1 - s0, 0), meshed(s1 - s0, 0);
                 for (int k = s0; k < s1; k++) {
                     const int j = k - s0;
-                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(Rv(), slot_f(a, a->seg, j), NS, a->dts_dev, k,
-                                                                ctx->ctl);
+                    // (the start state is already in its slot)
+                    emu::k_seg_save<<<g, emu::kBlock, 0, st>>>(Rv(), j == 0 ? nullptr : state_slot(i, k), NS,
+                                                                a->dts_dev, k, ctx->ctl);
                     const bool due = k + 1 < a->nsteps && (k + 1) % ri == 0;
                     if (k + 1 < s1 || due) {
                         // (the last step too when a re-sort follows it: its
@@ -1537,7 +1598,7 @@ int emu_adjoint_backward(emu_context* ctx, const double* lam_f_final, const doub
                 for (int k = s1 - 1; k >= s0; k--) {
                     const int j = k - s0;
                     if (has[j] && (r = move_static(a->gperm + (size_t)j * cap, true, true))) return r;
-                    G.seg = slot_f(a, a->seg, j);
+                    G.seg = state_slot(i, k);
                     G.k0 = k;
                     G.len = 1;
                     if (meshed[j]) {

@@ -155,15 +155,17 @@ def test_adjoint_errors():
 def test_adjoint_memory_modes_agree(monkeypatch, store):
     """every step stored by the recorded forward (no recompute), stage states
     recomputed and kept for a whole segment, recomputed step by step (budget
-    0), or step by step from sub-checkpoints every 2 or 3 steps inside a
-    7-step segment (the mode for runs whose checkpoints and step states would
-    not fit in memory): same gradient to rounding"""
+    0), or step by step from sub-checkpoints inside a 7-step segment held in
+    3 or 4 segment slots (sub-segments of 4 + 3 or 3 + 4 steps; the mode for
+    runs whose checkpoints and step states would not fit in memory): same
+    gradient to rounding"""
     if store == "segment":
         monkeypatch.setenv("EMU_ADJOINT_FULL_STORE", "0")
     elif store != "full":
         monkeypatch.setenv("EMU_ADJOINT_STORE_MAX_BYTES", "0")
     if store.startswith("per_step_sub"):
         monkeypatch.setenv("EMU_ADJOINT_SUBCHECKPOINT", store[-1])
+        monkeypatch.setenv("EMU_ADJOINT_SEG_SLOTS", str(int(store[-1]) + 1))
     p = W.c2_fast_flavor_1d(ncell_z=8, ndirs=6)
     parts = api.init_particles(p)
     fc, nc = flavor_columns(2), number_columns(2)
@@ -189,18 +191,20 @@ def test_adjoint_3d_resorted_every_step(monkeypatch, store):
     interval).  The recorded forward composes a segment's re-sorts into one
     map; the per-step modes re-sort their recomputes too and undo each step's
     permutation in the sweep, with the stage meshes kept from the state pass
-    (or, nomesh, redeposited by the sweep's recompute).  Gradient against
-    torch autograd."""
+    (or, nomesh, redeposited by the sweep's recompute); sub2: a 6-step
+    segment in 2 segment slots (sub-segments of 3, 2 and 1 steps).  Gradient
+    against torch autograd."""
     if store != "segment":
         monkeypatch.setenv("EMU_ADJOINT_STORE_MAX_BYTES", "0")
     if store.startswith("per_step_sub2"):
         monkeypatch.setenv("EMU_ADJOINT_SUBCHECKPOINT", "2")
+        monkeypatch.setenv("EMU_ADJOINT_SEG_SLOTS", "2")
     if store.endswith("nomesh"):
         monkeypatch.setenv("EMU_ADJOINT_STORE_MESHES", "0")
     p = W.c5_3d(n=3, ndirs=4, mixed=False)
     parts = api.init_particles(p)
     fc, nc = flavor_columns(3), number_columns(3)
-    with AdjointRun(p, parts, 7, 5) as run:
+    with AdjointRun(p, parts, 7, 6) as run:
         run.forward(parts[:, fc], parts[:, nc])
         J, lf, lN = run.ctx.adjoint_objective()
         g, gN = run.ctx.adjoint_backward(lf, lN)
