@@ -279,11 +279,12 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * EMU_ADJOINT_STORE_MAX_BYTES overrides it), else each step's stages are
  * recomputed before its backward step.  In that per-step mode the states of
  * every step of a segment are kept, or, when the checkpoints and those
- * states would not fit in the free device memory, sub-checkpoints every
- * J = ceil(sqrt(checkpoint_interval)) steps (J + interval / J states; each
- * step is recomputed once more; environment variable
- * EMU_ADJOINT_SUBCHECKPOINT sets J).  The context's particle state is
- * unchanged.
+ * states would not fit in the free device memory, sub-checkpoints inside
+ * a segment held in J + interval / J segment slots, J =
+ * ceil(sqrt(checkpoint_interval)) (each step is recomputed once more;
+ * environment variable EMU_ADJOINT_SUBCHECKPOINT sets J, and
+ * EMU_ADJOINT_SEG_SLOTS lowers the slot count, for tests).  The context's
+ * particle state is unchanged.
  *
  * emu_adjoint_reserve: allocates the checkpoint and work storage of a
  * recorded run of nsteps with this checkpoint_interval up front (what
