@@ -545,9 +545,8 @@ int emu_ctx::load_from_aos(emu_context* ctx, int64_t n, double pupt_min, const d
     ctx->loaded = true;
     ctx->adj_valid = false;
     ctx->steps_since_sort = 0;
-    if ((r = deposit_current(ctx))) return r;
-    CU(cudaStreamSynchronize(ctx->stream));
-    return EMU_OK;
+    // (asynchronous from here: the callers wait for what they need)
+    return deposit_current(ctx);
 }
 
 extern "C" {
@@ -606,6 +605,8 @@ int emu_create(const emu_params* p, emu_context** out)
     e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return bail(EMU_ERR_CUDA); }
     e = cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return bail(EMU_ERR_CUDA); }
+    e = cudaEventCreateWithFlags(&ctx->upload_done, cudaEventDisableTiming);
     if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return bail(EMU_ERR_CUDA); }
     ctx->stream = ctx->own;
     const size_t me = (size_t)mesh_elems(ctx);
@@ -671,6 +672,7 @@ void emu_destroy(emu_context* ctx)
     emu_ctx_comm_free(ctx);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->upload_done) cudaEventDestroy(ctx->upload_done);
     delete ctx;
 }
 
@@ -699,6 +701,7 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     if ((r = emu_ctx::reserve(ctx, n))) return r;
     CU(cudaMemcpyAsync(ctx->aos, records, sizeof(double) * (size_t)n * ctx->nreal, cudaMemcpyHostToDevice,
                        ctx->stream));
+    CU(cudaEventRecord(ctx->upload_done, ctx->stream));
     // scalars derived from the particles: Vvac_max (Init.cpp:657-660) and,
     // for the mixed path, the weight sums behind the fixed-point scales.  A
     // small set is scanned on the host while its copy is in flight; a large
@@ -711,7 +714,11 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
         for (int64_t q = 0; q < n; q++) pupt_min = std::min(pupt_min, records[q * ctx->nreal + 3 + 7]);
         if (ctx->mixed) emu_host::weight_totals(ctx->prm, records, n, tot, mx);
     }
-    return emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx);
+    if ((r = emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx))) return r;
+    // the caller may reuse the records (pinned memory is copied
+    // asynchronously): wait for the copy, not for the sort and deposit
+    CU(cudaEventSynchronize(ctx->upload_done));
+    return EMU_OK;
 }
 
 int emu_get_particles(emu_context* ctx, double* records, int64_t n)

@@ -23,6 +23,7 @@ struct emu_context {
     cudaStream_t stream = nullptr;      // where work is launched
     cudaStream_t own = nullptr;         // the context's own stream
     cudaStream_t cap_stream = nullptr;  // private stream used for graph capture
+    cudaEvent_t upload_done = nullptr;  // emu_load_particles: the records' copy has completed
     DevState S[2];                      // persistent particle arrays, double-buffered for re-sorts
     int cur = 0;                        // which of S[] is current
     void* pblock[2] = {nullptr, nullptr};

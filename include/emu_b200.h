@@ -161,7 +161,9 @@ int emu_set_stream(emu_context* ctx, void* cuda_stream);
 int emu_synchronize(emu_context* ctx);
 
 /* Upload particle records (host memory).  Replaces InitParticles/Restart as the
- * source of the container; particles are cell-sorted on the device. */
+ * source of the container; particles are cell-sorted on the device.  Returns
+ * once the records have been copied (the buffer may be reused); the sort and
+ * the deposit run on in the context's stream. */
 int emu_load_particles(emu_context* ctx, const double* records, int64_t n);
 /* Download particle records in load order. */
 int emu_get_particles(emu_context* ctx, double* records, int64_t n);
