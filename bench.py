@@ -370,6 +370,10 @@ def run_emu(args):
                "note": "per step of a batch: emu_load_particles from pinned host memory, emu_evolve_begin "
                        "(deposit + compute_dt), one device step, emu_get_particles to pinned host memory; "
                        "%d batches with their own contexts and host threads run concurrently" % pipes}
+        # its bound: pinned copies of the batch size, both directions at once
+        pc = pcie_copy_rate(bytes_rec, pipes)
+        pc["frac"] = e2e["value"] / n * bytes_rec / 1e9 / pc["concurrent_gbs_per_direction"]
+        e2e["pcie"] = pc
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -430,6 +434,39 @@ def run_emu(args):
         print(json.dumps(out))
     if torch.distributed.is_initialized():
         torch.distributed.destroy_process_group()
+
+
+def pcie_copy_rate(nbytes, nbuf, reps=10):
+    """GB/s of pinned host <-> device copies of nbytes (at most 256 MB),
+    nbuf copies per direction in flight: host to device alone, device to host
+    alone, and both at once on separate streams (per direction), the bound of
+    an end-to-end step that uploads and downloads a batch."""
+    import torch
+    nb = int(min(nbytes, 256 << 20))
+    nbuf = max(1, min(nbuf, int(1e9 // max(nb, 1))))
+    hs = [torch.empty(nb, dtype=torch.uint8).pin_memory() for _ in range(nbuf)]
+    hd = [torch.empty(nb, dtype=torch.uint8).pin_memory() for _ in range(nbuf)]
+    ds = [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(nbuf)]
+    dd = [torch.empty(nb, dtype=torch.uint8, device="cuda") for _ in range(nbuf)]
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def run(h2d, d2h):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            for i in range(nbuf):
+                if h2d:
+                    with torch.cuda.stream(sa):
+                        ds[i].copy_(hs[i], non_blocking=True)
+                if d2h:
+                    with torch.cuda.stream(sb):
+                        hd[i].copy_(dd[i], non_blocking=True)
+        torch.cuda.synchronize()
+        return nb * nbuf * reps / (time.perf_counter() - t0) / 1e9
+
+    run(True, True)   # warm-up
+    return {"h2d_gbs": run(True, False), "d2h_gbs": run(False, True),
+            "concurrent_gbs_per_direction": run(True, True), "bytes_per_copy": nb, "copies_in_flight": nbuf}
 
 
 def run_adjoint(ctx, recs, p, stream, fwd_ms_per_step, nsteps, interval):
