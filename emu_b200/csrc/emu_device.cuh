@@ -266,10 +266,15 @@ struct SW {
 };
 
 
-__device__ __forceinline__ void atomic_add_mesh(double* p, double v) { atomicAdd(p, v); }
+// mesh sums: global-memory reductions without a returned value (the mesh is
+// always global memory: context, adjoint and static meshes)
+__device__ __forceinline__ void atomic_add_mesh(double* p, double v)
+{
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
 __device__ __forceinline__ void atomic_add_mesh(long long* p, long long v)
 {
-    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 // ---------------------------------------------------------------------------
