@@ -285,7 +285,9 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
  * a segment held in J + interval / J segment slots, J =
  * ceil(sqrt(checkpoint_interval)) (each step is recomputed once more;
  * environment variable EMU_ADJOINT_SUBCHECKPOINT sets J, and
- * EMU_ADJOINT_SEG_SLOTS lowers the slot count, for tests).  The context's
+ * EMU_ADJOINT_SEG_SLOTS lowers the slot count, for tests).  With re-sorts,
+ * the per-step mode also keeps each step's stage meshes when the free
+ * memory allows (EMU_ADJOINT_STORE_MESHES=0 turns that off).  The context's
  * particle state is unchanged.
  *
  * emu_adjoint_reserve: allocates the checkpoint and work storage of a
