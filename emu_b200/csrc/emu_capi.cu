@@ -709,15 +709,21 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n)
     // over the records).
     double pupt_min = INFINITY, tot[2] = {0, 0}, mx[2] = {0, 0};
     if (n > kHostStatsMax) {
-        if ((r = emu_ctx::record_stats(ctx, n, pupt_min, tot, mx))) return r;
+        if ((r = emu_ctx::record_stats(ctx, n, pupt_min, tot, mx))) {
+            cudaEventSynchronize(ctx->upload_done);   // (the records stay in use until copied)
+            return r;
+        }
     } else {
         for (int64_t q = 0; q < n; q++) pupt_min = std::min(pupt_min, records[q * ctx->nreal + 3 + 7]);
         if (ctx->mixed) emu_host::weight_totals(ctx->prm, records, n, tot, mx);
     }
-    if ((r = emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx))) return r;
+    r = emu_ctx::load_from_aos(ctx, n, pupt_min, tot, mx);
     // the caller may reuse the records (pinned memory is copied
-    // asynchronously): wait for the copy, not for the sort and deposit
-    CU(cudaEventSynchronize(ctx->upload_done));
+    // asynchronously): wait for the copy, not for the sort and deposit, and
+    // on the error paths too
+    const cudaError_t e = cudaEventSynchronize(ctx->upload_done);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("emu_load_particles: ") + cudaGetErrorString(e));
     return EMU_OK;
 }
 
