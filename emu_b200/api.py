@@ -24,6 +24,7 @@ EMU_ERR_IO = 128
 EMU_ERR_PARSE = 256
 EMU_ERR_NOMEM = 512
 EMU_ERR_LIMIT = 1024
+EMU_ERR_TIMEOUT = 2048
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -120,6 +121,7 @@ SIGNATURES = {
     "emu_evolve_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "emu_evolve_end": (ctypes.c_int, [ctypes.c_void_p, _P(EmuRunInfo)]),
     "emu_flush_l2": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
+    "emu_set_wait_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
     "emu_profile_step": (ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_float), ctypes.c_int, _P(ctypes.c_int)]),
     "emu_write_plotfile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int,
                                           ctypes.c_int]),
@@ -190,11 +192,37 @@ def _check(code, ctx=None, what=""):
 
 
 def default_params(**kw):
+    """emu_params with the defaults of emu_params_default, set here without
+    loading the library (the host-only benchmark legs build their workloads
+    from these; tests pin the two byte for byte)."""
+    p = EmuParams()
+    ctypes.memset(ctypes.byref(p), 0, ctypes.sizeof(EmuParams))
+    p.nflavors, p.shape_order, p.precision = 2, 2, PREC_FP64
+    p.integration_type, p.rk_type = 1, 4
+    for d in range(3):
+        p.ncell[d] = 1
+        p.nppc[d] = 1
+    p.nphi_equator = 1
+    p.Lx = p.Ly = p.Lz = 1.0
+    p.max_grid_size = 64
+    p.nsteps = 1
+    p.end_time = 1.0
+    p.write_plot_every = p.write_plot_particles_every = 1
+    p.T_in, p.Ye_in = 10.0, 1.0
+    p.cfl_factor = p.flavor_cfl_factor = 0.5
+    p.maxError = 1e-6
+    p.direction_generator, p.ndirections, p.seed = 0, 0, 0
+    p.resort_interval, p.fused = -1, 1
+    for k, v in kw.items():
+        set_param(p, k, v)
+    return p
+
+
+def library_default_params():
+    """emu_params_default of the library itself"""
     lib = load_library()
     p = EmuParams()
     lib.emu_params_default(ctypes.byref(p))
-    for k, v in kw.items():
-        set_param(p, k, v)
     return p
 
 
@@ -429,6 +457,11 @@ class Context:
         nk = ctypes.c_int(0)
         self._ck(self.lib.emu_profile_step(self.h, buf, 16, ctypes.byref(nk)), "emu_profile_step")
         return [buf[i] for i in range(nk.value)]
+
+    def set_wait_limit(self, polls):
+        """limit of the cooperative kernels' grid-barrier waits (polls; < 0:
+        the default)"""
+        self._ck(self.lib.emu_set_wait_limit(self.h, int(polls)), "emu_set_wait_limit")
 
     def flush_l2(self, ptr, nbytes):
         self._ck(self.lib.emu_flush_l2(self.h, ctypes.c_void_p(ptr), int(nbytes)), "emu_flush_l2")

@@ -51,6 +51,7 @@ void emu::make_devparams(const emu_params& p, DevParams& P)
 {
     std::memset(&P, 0, sizeof(P));
     P.nf = p.nflavors;
+    P.wait_polls = kBarrierSpins;
     double L[3] = {p.Lx, p.Ly, p.Lz};
     double dx[3];
     for (int d = 0; d < 3; d++) {
@@ -929,6 +930,13 @@ int emu_evolve(emu_context* ctx, int nsteps, double start_time, double end_time,
     return emu_evolve_end(ctx, info);
 }
 
+int emu_set_wait_limit(emu_context* ctx, int64_t polls)
+{
+    if (!ctx) return EMU_ERR_ARG;
+    ctx->P.wait_polls = polls < 0 ? emu::kBarrierSpins : (long long)polls;
+    return EMU_OK;
+}
+
 int emu_flush_l2(emu_context* ctx, void* buf, int64_t bytes)
 {
     if (!ctx || !buf) return EMU_ERR_ARG;
@@ -964,8 +972,10 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
         return EMU_OK;
     }
     const int nk = ctx->mixed ? 8 : 4;
-    if (max_kernels < nk) return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
-    std::vector<cudaEvent_t> ev(2 * nk);
+    const bool resort_due = ctx->prm.resort_interval > 0 && ctx->steps_since_sort + 1 >= ctx->prm.resort_interval;
+    if (max_kernels < nk + (resort_due ? 1 : 0))
+        return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
+    std::vector<cudaEvent_t> ev(2 * nk + 2);
     for (auto& e : ev) CU(cudaEventCreate(&e));
     const DevState& S = ctx->S[ctx->cur];
     cudaStream_t st = ctx->stream;
@@ -1004,12 +1014,19 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
     int r = check_launch(ctx, "profile step");
     if (r) return r;
     ctx->cur_mesh = ctx->mixed ? 1 : 3;
+    if (ctx->prm.resort_interval > 0) ctx->steps_since_sort++;
+    if (resort_due) {
+        // the re-sort that follows the step (keys, radix sort, gather) as
+        // one more entry
+        rec(2 * k);
+        if ((r = resort(ctx))) return r;
+        rec(2 * k + 1);
+        k++;
+    }
     CU(cudaStreamSynchronize(st));
     for (int i = 0; i < k; i++) CU(cudaEventElapsedTime(&kernel_ms[i], ev[2 * i], ev[2 * i + 1]));
     for (auto& e : ev) cudaEventDestroy(e);
     *nkernels = k;
-    if (ctx->prm.resort_interval > 0 && ++ctx->steps_since_sort >= ctx->prm.resort_interval)
-        if ((r = resort(ctx))) return r;
     return EMU_OK;
 }
 

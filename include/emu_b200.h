@@ -36,7 +36,7 @@ extern "C" {
 #define EMU_ERR_TRACE    1     /* Renormalize: |trace-1| > 100*maxError   (generate_code.py:404-409) */
 #define EMU_ERR_NEGDIAG  2     /* Renormalize: diagonal < -100*maxError  (generate_code.py:418-423) */
 #define EMU_ERR_LENGTH   4     /* Renormalize: |length-L| > 100*maxError  (generate_code.py:433-438) */
-#define EMU_ERR_DT       8     /* compute_dt: no limiter active           (Evolve.cpp:119-121) */
+#define EMU_ERR_DT       8     /* compute_dt: no limiter active           (Evolve.cpp:76-86)  */
 #define EMU_ERR_ARG      16    /* invalid argument */
 #define EMU_ERR_CUDA     32    /* CUDA runtime failure (no device, launch error, ...) */
 #define EMU_ERR_STATE    64    /* call out of order (e.g. no particles loaded) */
@@ -169,17 +169,17 @@ int emu_load_particles(emu_context* ctx, const double* records, int64_t n);
 int emu_get_particles(emu_context* ctx, double* records, int64_t n);
 int emu_num_particles(const emu_context* ctx, int64_t* n);
 
-/* deposit_to_mesh (Evolve.H:31 / Evolve.cpp:126-161) of the current particles */
+/* deposit_to_mesh (Evolve.H:31 / Evolve.cpp:91-126) of the current particles */
 int emu_deposit(emu_context* ctx);
 /* The current mesh (rho,T,Ye and the last deposit), GIdx planes. */
 int emu_get_mesh(emu_context* ctx, double* out);
-/* interpolate_rhs_from_mesh (Evolve.H:33 / Evolve.cpp:163-211): the time
+/* interpolate_rhs_from_mesh (Evolve.H:33 / Evolve.cpp:128-176): the time
  * derivative of every attribute of every particle, from the current mesh,
  * written as particle records in load order (positions copied through). */
 int emu_interpolate_rhs(emu_context* ctx, double* rhs_records);
 /* FlavoredNeutrinoContainer::Renormalize (FlavoredNeutrinoContainer.H:92). */
 int emu_renormalize(emu_context* ctx, int64_t* bad_particle);
-/* compute_dt (Evolve.H:29 / Evolve.cpp:57-124) on the current mesh. */
+/* compute_dt (Evolve.H:29 / Evolve.cpp:22-89) on the current mesh. */
 int emu_compute_dt(emu_context* ctx, double* dt);
 /* One integrator step of length dt (TimeIntegrator::advance with
  * ApplyFlavoredNeutrinoRHS, FlavoredNeutrinoContainer.H:33-47) followed by the
@@ -199,14 +199,25 @@ int emu_evolve(emu_context* ctx, int nsteps, double start_time, double end_time,
 int emu_evolve_begin(emu_context* ctx, double start_time, double end_time, int max_steps);
 int emu_evolve_steps(emu_context* ctx, int nsteps);
 int emu_evolve_end(emu_context* ctx, emu_run_info* info);
+/* Limit of the bounded grid-barrier waits of this context's cooperative
+ * kernels (the whole-step kernel of fused = 2 and the adjoint's segment
+ * kernels), in polls of a 64 ns sleep; polls < 0 restores the default
+ * (2^22).  A wait that runs out sets EMU_ERR_TIMEOUT in the run's status and
+ * lets the kernel finish (the step's results are then invalid); the next
+ * emu_evolve_begin or emu_load_particles resets the barrier.  No
+ * counterpart in the reference (its steps have no device-side waits);
+ * tests use a limit of 0 to make a wait run out. */
+int emu_set_wait_limit(emu_context* ctx, int64_t polls);
 /* Overwrite a device buffer (bytes, multiple of 8) on the context's stream;
  * benchmarks use it to evict the L2 cache between timed steps. */
 int emu_flush_l2(emu_context* ctx, void* device_buffer, int64_t bytes);
 /* One device-resident step (as emu_evolve_steps(ctx, 1)) launched kernel by
  * kernel with a CUDA event pair around each launch on the context stream.
  * kernel_ms[i] receives the duration of kernel i in launch order (the RK
- * stages, then the compute_dt reduction); *nkernels their count.  Call after
- * emu_evolve_begin. */
+ * stages, with the mixed path's finalize kernel before each; stage 4 also
+ * reduces compute_dt), then, when a re-sort follows the step, the whole
+ * re-sort (keys, radix sort, gather) as one more entry; *nkernels their
+ * count (at most 9).  Call after emu_evolve_begin. */
 int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* nkernels);
 
 /* Plotfile (IO.cpp:11-38): mesh plotfile pltNNNNN plus, when
@@ -227,24 +238,26 @@ int emu_last_error(const emu_context* ctx, char* buf, size_t len);
 /*
  * deposit_to_mesh for callers that cannot allocate device memory.  No
  * counterpart in the reference: its deposit writes into an AMReX MultiFab
- * the caller already owns.  Some callers cannot call cudaMalloc when they
- * need a deposit (work being captured into a CUDA graph, a fixed memory pool
- * handed over at start-up, a loop that must not touch the allocator); this
- * entry point allocates nothing.  Inputs and outputs are device memory owned
- * by the caller:
+ * the caller already owns.  Some host programs cannot let a library call
+ * cudaMalloc: one that hands all device memory to its own pool allocator at
+ * start-up has nothing left to allocate from, and a time-critical step loop
+ * cannot afford cudaMalloc/cudaFree (cudaFree synchronises the whole
+ * device).  This entry point allocates nothing.  Inputs and outputs are
+ * device memory owned by the caller:
  *   d_records   n particle records (rows of emu_nreal(nflavors) FP64, the
- *               emu_load_particles layout), on the device
+ *               emu_load_particles layout, in any order), on the device
  *   d_mesh_out  emu_ncomp(nflavors) x ncells FP64 in emu_get_mesh layout
  * Its only scratch, the cell-major accumulation mesh, is a fixed array of
  * 2^19 doubles (4 MiB) compiled into the library; ncells * 8 * nflavors^2
  * must not exceed it (EMU_ERR_LIMIT otherwise).  Every GPU that loads the
- * library keeps the array until the process exits.  The first call on a
- * device looks up the array's device address once (cudaGetSymbolAddress);
- * make that first call before any stream capture.  All calls share the
- * array and each call clears it first, so calls that overlap on the GPU
- * (different streams, threads or processes on one device) race and must be
- * serialised by the caller.  Work is enqueued on `stream` (a cudaStream_t,
- * NULL = the legacy default stream); the call does not synchronise.
+ * library keeps the array until the process exits.  The first call in a
+ * device context (and again after a device reset) looks up the array's
+ * device address with cudaGetSymbolAddress, with that device current; make
+ * that first call before any stream capture.  All calls share the array and
+ * each call clears it first, so calls that overlap on the GPU (different
+ * streams, threads or processes on one device) race and must be serialised
+ * by the caller.  Work is enqueued on `stream` (a cudaStream_t, NULL = the
+ * legacy default stream); the call does not synchronise.
  * Errors: emu_last_error(NULL, ...).
  */
 int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n, double* d_mesh_out,
