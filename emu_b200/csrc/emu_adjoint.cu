@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
         for (int s = 1; s <= 3; s++) {
             adj_fwd_stage_body<NF, SWt>(P, Q, s, dt, s == 1 ? Y0 : seg_y(G, j, s, cap), Y0, G.acc,
                                         seg_y(G, j, s + 1, cap), seg_m(G, j, s - 1), seg_m(G, j, s));
-            grid_barrier(ctl);
+            grid_barrier(ctl, P.wait_polls);
         }
         // recording: compute_dt on the stage-4 mesh (main.cpp:193-198), the
         // next step's dt; M_4 is complete and every block holds this step's
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_fwd_coop(DevParams P, Dev
                                           next ? seg_f(G, j + 1) : nullptr,
                                           next ? seg_f(G, j + 1) + (long long)G.NS * cap : nullptr, seg_m(G, j, 3),
                                           more ? seg_m(G, j + 1, 0) : nullptr, G.record ? ctl : nullptr);
-        grid_barrier(ctl);
+        grid_barrier(ctl, P.wait_polls);
         if (G.record && __ldcg(&ctl->done) && more) break;   // (uniform: read after the barrier)
     }
 }
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_adj_seg_bwd_coop(DevParams P, Dev
 #pragma unroll 1
         for (int s = 4; s >= 0; s--) {
             adj_stage_body<NF, SWt>(P, Q, s, dt, seg_stage_ptrs(G, j, s, cap));
-            grid_barrier(ctl);
+            grid_barrier(ctl, P.wait_polls);
         }
     }
 }

@@ -5,9 +5,9 @@
 //
 // Reference semantics (paths relative to the Emu tree):
 //   shape factors        Source/ParticleInterpolator.H:34-131
-//   deposit              Source/Evolve.cpp:126-161, generate_code.py:150-169
-//   potentials           Source/Evolve.cpp:163-193, generate_code.py:239-357
-//   commutator RHS       Source/Evolve.cpp:195-210, generate_code.py:359-389
+//   deposit              Source/Evolve.cpp:91-126, generate_code.py:150-169
+//   potentials           Source/Evolve.cpp:128-158, generate_code.py:239-357
+//   commutator RHS       Source/Evolve.cpp:160-174, generate_code.py:359-389
 //   Renormalize          Source/FlavoredNeutrinoContainer.cpp:89-113,
 //                        generate_code.py:391-445
 #pragma once
@@ -63,7 +63,7 @@ struct DevParams {
     double g_scale, g_unscale;   // fixed point of the mixed path's self-interaction mesh (both species)
     double L[3];       // domain length (periodic, [0,L))
     double dxi[3];     // inverse cell size
-    double sqrt2GF_inv_vol;   // sqrt(2)*GF*inv_cell_volume (Evolve.cpp:167 + fill)
+    double sqrt2GF_inv_vol;   // sqrt(2)*GF*inv_cell_volume (Evolve.cpp:132 + fill)
     double matter;            // rho*Ye/Mp/inv_cell_volume (uniform background)
     double M2[2][9];          // vacuum mass-squared matrix, nu and nubar (conjugated)
     double c4;                // c^4
@@ -80,6 +80,7 @@ struct DevParams {
     // turns an integer mesh sum back into sqrt(2) GF n (erg)
     double q_scale[2];        // contribution * q_scale -> integer
     double q_unscale[2];      // integer * q_unscale -> number (same units as FP64 mesh)
+    long long wait_polls;     // polls of a grid-barrier wait before it gives up (ST_TIMEOUT)
 };
 
 // ---------------------------------------------------------------------------

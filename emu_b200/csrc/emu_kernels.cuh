@@ -1,5 +1,6 @@
 // emu_kernels.cuh -- device data layout and the host-side launchers of the
-// evolution kernels (implemented in emu_kernels.cu).
+// evolution kernels (implemented in emu_kernels_impl.cuh, instantiated in
+// emu_k_fp64_<nf>.cu, emu_k_mixed_<nf>.cu and emu_k_misc.cu).
 //
 // HBM layout (structure of arrays, particles cell-sorted, stride = cap):
 //   pos[3], time, pup[4], Nn[2] (N, Nbar), Ll[2] (L, Lbar)        FP64
@@ -69,6 +70,8 @@ struct StepCtl {
 enum DtMode : int { DT_QUERY = 0, DT_INIT = 1, DT_ADVANCE = 2 };
 
 constexpr int kBlock = 128;
+// default limit of a grid-barrier wait (polls of 64 ns sleeps, ~0.3 s or more)
+constexpr long long kBarrierSpins = 1ll << 22;
 
 // launchers (all asynchronous on the given stream)
 void launch_pack(int nf, const DevParams& P, const double* aos, const unsigned* perm, long long n, DevState S,

@@ -57,7 +57,7 @@ inline unsigned grid_for(long long n, int block = kBlock)
     }
 
 // ---------------------------------------------------------------------------
-// FP64 potential of one particle (Evolve.cpp:163-193 with the Vvac and
+// FP64 potential of one particle (Evolve.cpp:128-158 with the Vvac and
 // interpolate fills): V starts at the vacuum term and accumulates
 // coef*inside per stencil cell, nubar with the reference's sign rule.
 template <int NF, class SWt>
@@ -197,7 +197,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 }
 
 // ===========================================================================
-// compute_dt pieces (Evolve.cpp:57-124 + compute_dt fill)
+// compute_dt pieces (Evolve.cpp:22-89 + compute_dt fill)
 // ===========================================================================
 __device__ __forceinline__ void block_max2(double& a, double& b)
 {
@@ -944,12 +944,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_stage(DevParams P, DevState S
 }
 
 // Grid-wide barrier of the cooperative step kernel (its CTAs are co-resident
-// by cooperative launch).  The wait is bounded: after kBarrierSpins polls the
-// CTA records ST_TIMEOUT in the step status and continues, so a failure can
-// never hang the GPU.
-constexpr long long kBarrierSpins = 1ll << 22;
-
-__device__ __forceinline__ void grid_barrier(StepCtl* ctl)
+// by cooperative launch).  The wait is bounded: after `polls` polls (64 ns
+// sleeps; DevParams::wait_polls, kBarrierSpins unless a caller set another
+// limit) the CTA records ST_TIMEOUT in the step status and continues, so a
+// failure can never hang the GPU.  The results of a step that timed out are
+// invalid; every memory index of the step is computed from wrapped
+// positions and CTA-local ranks, so they stay in bounds whatever the data.
+__device__ __forceinline__ void grid_barrier(StepCtl* ctl, long long polls)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -963,7 +964,7 @@ __device__ __forceinline__ void grid_barrier(StepCtl* ctl)
         } else {
             long long it = 0;
             while (*genp == g) {
-                if (++it > kBarrierSpins) {
+                if (++it > polls) {
                     atomicOr(&ctl->status, ST_TIMEOUT);
                     break;
                 }
@@ -992,7 +993,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_rk4_step_coop(DevParams P, DevSta
 #pragma unroll 1
     for (int s = 1; s <= 4; s++) {
         rk4_stage_body<NF, SWt>(P, S, s, m[s - 1], m[s % 4], m[(s + 1) % 4], nmesh, ctl, dt);
-        if (s < 4) grid_barrier(ctl);
+        if (s < 4) grid_barrier(ctl, P.wait_polls);
     }
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, m3, ctl, DT_ADVANCE, reduce_blocks(P));
 }
@@ -1013,7 +1014,7 @@ __global__ void __launch_bounds__(2 * kBlock, 2) k_rk4_step_coop_split(DevParams
 #pragma unroll 1
     for (int s = 1; s <= 4; s++) {
         rk4_stage_body_split<NF, SWt>(P, S, s, m[s - 1], m[s % 4], m[(s + 1) % 4], nmesh, ctl, dt);
-        if (s < 4) grid_barrier(ctl);
+        if (s < 4) grid_barrier(ctl, P.wait_polls);
     }
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, double>(P, m3, ctl, DT_ADVANCE, reduce_blocks(P));
 }
@@ -1355,6 +1356,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     }
     grid_dep_wait();
     grid_dep_launch();
+    bool live = active;   // false: this particle's staged state never arrived
     if constexpr (STAGE) {
         if (s > 1 && t < 32)
             for (int c = t; c < 2 * NS; c += 32) {
@@ -1393,11 +1395,17 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         const double w6 = dt * (1.0 / 6.0);
         int stt = 0;
         if constexpr (STAGE) {
-            if (!mbar_wait(&stage_bar, 0)) atomicOr(&ctl->status, ST_TIMEOUT);
+            // a thread whose wait gives up reads none of the staged state
+            // and writes nothing of its particle (the step is invalid)
+            if (!mbar_wait(&stage_bar, 0)) {
+                atomicOr(&ctl->status, ST_TIMEOUT);
+                live = false;
+            }
         }
         // one species at a time keeps the live state small
 #pragma unroll
         for (int sp = 0; sp < 2; sp++) {
+            if (!live) break;
             double y0[NH], f[NH];
 #pragma unroll
             for (int e = 0; e < NH; e++) {
@@ -1454,7 +1462,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
 #pragma unroll
             for (int e = 0; e < NH; e++) fN[sp * NH + e] = (float)fn[e] * Ns;
         }
-        if (s == 4) {
+        if (s == 4 && live) {
             double xn[3] = {x, y, z};
             double tn = PRELOAD ? t_in : s4[t];
             const double pq[4] = {PRELOAD ? pu[0] : s4[kBlock + t], PRELOAD ? pu[1] : s4[2 * kBlock + t],
@@ -1480,9 +1488,13 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     }
     if constexpr (STAGE) {
         // the staged state is consumed (and the copies complete) before the
-        // deposit records reuse the area
-        if (t == 0 && !mbar_wait(&stage_bar, 0)) atomicOr(&ctl->status, ST_TIMEOUT);
-        __syncthreads();
+        // deposit records reuse the area; when the copies do not complete
+        // within the bounded wait the CTA deposits nothing
+        const bool drained = __syncthreads_and(t != 0 || mbar_wait(&stage_bar, 0));
+        if (!drained) {
+            if (t == 0) atomicOr(&ctl->status, ST_TIMEOUT);
+            return;
+        }
     }
     if (qout) {
         // (stages 1-3: the rank the last stage 4 stored, see rk4_stage_body)
@@ -1490,14 +1502,14 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         if (s == 3) {
             // M_4, the mesh compute_dt reads (N, Nbar and the fluxes apart):
             // the full layout
-            tile_deposit_block<NF, SWt, float>(P, qout, active, st, fN, vx, vy, vz, QuantConv{P}, false, given);
+            tile_deposit_block<NF, SWt, float>(P, qout, live, st, fN, vx, vy, vz, QuantConv{P}, false, given);
         } else {
             // M_2, M_3 and the next step's M_1: only the combinations the
             // stages interpolate
             float cN[NH];
             combine_species<NF>(fN, cN);
             const int sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(
-                P, qout, active, st, cN, vx, vy, vz, QuantConvG{P}, s == 4, given);
+                P, qout, live, st, cN, vx, vy, vz, QuantConvG{P}, s == 4, given);
             if (s == 4 && active) S.rslot[p] = sl;
         }
     }
@@ -1553,7 +1565,7 @@ __global__ void k_unpack(DevState S, double* __restrict__ aos)
     }
 }
 
-// derivative records (interpolate_rhs_from_mesh output, Evolve.cpp:195-210)
+// derivative records (interpolate_rhs_from_mesh output, Evolve.cpp:160-174)
 template <int NF>
 __global__ void k_unpack_rhs(DevState S, const double* __restrict__ K, double* __restrict__ aos)
 {
