@@ -208,7 +208,7 @@ static bool mkdir_p(const std::string& d)
 
 std::vector<std::string> grid_names(int nf)
 {
-    // Evolve.cpp:43-54 + generated grid_names fill
+    // GIdx::Initialize (Evolve.cpp:8-20) + generated grid_names fill
     std::vector<std::string> names = {"rho", "T", "Ye"};
     const char* vars[4] = {"N", "Fx", "Fy", "Fz"};
     const char* tails[2] = {"", "bar"};

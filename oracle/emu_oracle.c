@@ -140,7 +140,7 @@ static int imod(int a, int n)
     return r < 0 ? r + n : r;
 }
 
-/* per-dimension shape order: 0 for one-cell dimensions (Evolve.cpp:137-139) */
+/* per-dimension shape order: 0 for one-cell dimensions (Evolve.cpp:102-104, 134-136) */
 static void dim_orders(const oracle_params* P, int ord[3])
 {
     for (int d = 0; d < 3; d++) ord[d] = P->ncell[d] > 1 ? P->shape_order : 0;
@@ -176,7 +176,7 @@ void oracle_init_mesh(const oracle_params* P, double* mesh)
 static int gidx(int nf, int dir, int s, int e) { return 3 + (dir * 2 + s) * nf * nf + e; }
 
 /* deposit of a particle slice into an accumulation mesh (deposited comps only)
- * Evolve.cpp:126-161 and generate_code.py:150-169.  The reference deposits
+ * Evolve.cpp:91-126 and generate_code.py:150-169.  The reference deposits
  * into ghost cells and folds them back with SumBoundary; with periodic
  * boundaries that equals accumulating into (index mod ncell). */
 static void deposit_slice(const oracle_params* P, const double* parts, int64_t lo, int64_t hi,
@@ -383,7 +383,7 @@ static void commutator_rhs(int nf, const double* h, const double* f, double* out
         }
 }
 
-/* interpolate_rhs_from_mesh for one particle: Evolve.cpp:163-211 and the
+/* interpolate_rhs_from_mesh for one particle: Evolve.cpp:128-176 and the
  * Vvac / interpolate / dfdt fills (generate_code.py:239-255, 296-389). */
 static void interp_one(const oracle_params* P, const double* mesh, const double* pp, double* out,
                        const double* Vvac_unit)
@@ -434,7 +434,7 @@ static void interp_one(const oracle_params* P, const double* mesh, const double*
                 }
             }
 
-    /* non-flavor derivatives (Evolve.cpp:196-207) */
+    /* non-flavor derivatives (Evolve.cpp:160-172) */
     out[0] = pp[0];
     out[1] = pp[1];
     out[2] = pp[2];
@@ -546,7 +546,7 @@ void oracle_wrap(const oracle_params* P, double* parts, int64_t n)
     }
 }
 
-/* compute_dt: Evolve.cpp:57-124 and generate_code.py:257-294 */
+/* compute_dt: Evolve.cpp:22-89 and generate_code.py:257-294 */
 int oracle_compute_dt(const oracle_params* P, const double* mesh, double vvac_max, double* dt_out)
 {
     const int nf = P->nflavors, nh = nf * nf;

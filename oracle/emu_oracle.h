@@ -90,7 +90,7 @@ int oracle_renormalize(const oracle_params* P, double* parts, int64_t n,
 /* periodic wrap of positions + SyncLocation (main.cpp:163-170) */
 void oracle_wrap(const oracle_params* P, double* parts, int64_t n);
 
-/* compute_dt (Evolve.cpp:57-124) from a deposited mesh */
+/* compute_dt (Evolve.cpp:22-89) from a deposited mesh */
 int oracle_compute_dt(const oracle_params* P, const double* mesh,
                       double vvac_max, double* dt);
 

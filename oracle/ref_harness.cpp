@@ -125,7 +125,7 @@ static Geo make_geo(const oracle_params* P)
     Geo g;
     Real L[3] = {P->Lx, P->Ly, P->Lz};
     for (int d = 0; d < 3; d++) {
-        g.ord[d] = P->ncell[d] > 1 ? P->shape_order : 0;         /* Evolve.cpp:137-139 */
+        g.ord[d] = P->ncell[d] > 1 ? P->shape_order : 0;         /* Evolve.cpp:102-104, 134-136 */
         g.ngrow[d] = 1 + (1 + (P->ncell[d] == 1 ? 0 : P->shape_order)) / 2;  /* main.cpp:68-71 */
         g.dx[d] = L[d] / (Real)P->ncell[d];
         g.dxi[d] = 1.0 / g.dx[d];
@@ -183,7 +183,7 @@ static void mesh_from_fab(const Fab& F, const oracle_params* P, double* mesh, in
                     mesh[c * nc + ((int64_t)k * P->ncell[1] + j) * P->ncell[0] + i] = F.v[F.at(i, j, k, c)];
 }
 
-/* ---- deposit_to_mesh (Evolve.cpp:126-161) ---- */
+/* ---- deposit_to_mesh (Evolve.cpp:91-126) ---- */
 static void deposit_range(const Geo& g, const double* parts, int64_t lo, int64_t hi, Fab& F)
 {
     const auto plo = g.plo;
@@ -224,7 +224,7 @@ extern "C" void ref_deposit(const oracle_params* P, const double* parts, int64_t
     mesh_from_fab(fabs[0], P, mesh, GIdx::N00_Re);
 }
 
-/* ---- interpolate_rhs_from_mesh (Evolve.cpp:163-211) ---- */
+/* ---- interpolate_rhs_from_mesh (Evolve.cpp:128-176) ---- */
 static void interpolate_fab(const oracle_params* P, const Fab& F, const double* parts, int64_t n,
                             double* out, int nthreads)
 {
@@ -320,7 +320,7 @@ extern "C" double ref_vvac_max(const oracle_params* P, const double* parts, int6
     return Vvac_max;
 }
 
-/* ---- compute_dt (Evolve.cpp:57-124), reduction over the grown box ---- */
+/* ---- compute_dt (Evolve.cpp:22-89), reduction over the grown box ---- */
 extern "C" int ref_compute_dt(const oracle_params* P, const double* mesh, double vvac_max, double* dt_out)
 {
     Fab F;

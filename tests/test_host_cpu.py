@@ -10,10 +10,13 @@ import pytest
 
 from emu_b200 import api
 from emu_b200 import workloads as W
+from oracle.build_oracle import REF_ROOT
 from oracle.oracle import Oracle
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INPUTS = "/root/reference/sample_inputs"
+# the reference's sample inputs files, where the reference tree is present
+# (the oracle build recipe's EMU_REFERENCE_ROOT)
+REF_INPUTS = os.path.join(REF_ROOT, "sample_inputs")
 
 
 def declared_symbols():

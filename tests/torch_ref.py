@@ -3,7 +3,7 @@ infrastructure): the gradient of its objective by torch autograd is the
 reference for the library's hand-written adjoint.
 
 Same semantics as the oracle (deposit_to_mesh Evolve.cpp:91-126,
-interpolate_rhs_from_mesh Evolve.cpp:128-211 with the generated fills,
+interpolate_rhs_from_mesh Evolve.cpp:128-176 with the generated fills,
 Renormalize generate_code.py:391-445, RK4 main.cpp:129-203), written with
 differentiable torch operations on the flavor state and the N weights.
 Stencils, vacuum potentials and positions are not differentiated; the
