@@ -67,6 +67,9 @@ int main(int argc, char** argv)
         recs.resize((size_t)n * emu_nreal(p.nflavors));
         if ((r = emu_read_particles(p.restart_dir, p.nflavors, recs.data(), n, &n, &t0, &step0)))
             return die(nullptr, r, "restart");
+        // (IO.cpp:61)
+        std::printf("Restarting after time step: %d t = %.17g s.  ct = %.17g cm\n", step0 - 1, t0,
+                    2.99792458e10 * t0);
     }
     emu_context* ctx = nullptr;
     if ((r = emu_create(&p, &ctx))) return die(nullptr, r, "emu_create");

@@ -98,3 +98,39 @@ def test_driver_runs_inputs_and_writes_plotfiles(tmp_path):
     # override on the command line: 2 steps, no plotfiles after the first
     r = _run([str(f), "nsteps=2", "write_plot_every=100", "write_plot_particles_every=0"], tmp_path / ".")
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_restart_continues_like_the_reference(tmp_path):
+    """do_restart = 1 (main.cpp:103-110, RecoverParticles IO.cpp:40-63): the
+    run restarted from plt00003 takes the particles, time and step of that
+    plotfile, deposits them and takes its first dt from that mesh, as the
+    reference's restart does; its plt00006 equals the oracle continuing
+    from plt00003 the same way (1e-12), and the uninterrupted run (whose dt
+    after step 3 came from the stage-4 mesh) to 1e-6."""
+    from oracle.oracle import Oracle
+    full, rest = tmp_path / "full", tmp_path / "restart"
+    full.mkdir()
+    rest.mkdir()
+    f = tmp_path / "inputs"
+    f.write_text(FAST_FLAVOR)
+    r = _run([str(f), "nsteps=6"], full)
+    assert r.returncode == 0, r.stderr
+    r = _run([str(f), "nsteps=6", "do_restart=1", "restart_dir=%s" % (full / "plt00003")], rest)
+    assert r.returncode == 0, r.stderr
+    assert "Restarting after time step: 2 t = " in r.stdout
+    assert not (rest / "plt00000").exists() and not (rest / "plt00003").exists()
+    p = api.parse_inputs(str(f))
+    p3, t3, s3 = api.read_particles(str(full / "plt00003"), 2)
+    assert s3 == 3
+    out, t, step = api.read_particles(str(rest / "plt00006"), 2)
+    assert step == 6
+    ref, t_ref, _, st = Oracle(p).evolve(p3, 3, start_time=t3)
+    assert st == 0 and abs(t - t_ref) <= 1e-13 * t_ref
+    key = lambda a: np.lexsort((a[:, 9], a[:, 8], a[:, 7], a[:, 2], a[:, 1], a[:, 0]))
+    a, b = out[key(out)], ref[key(ref)]
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+    u, tu, _ = api.read_particles(str(full / "plt00006"), 2)
+    assert abs(tu - t) <= 1e-6 * t
+    uu = u[key(u)]
+    assert np.abs(uu[:, 3:] - a[:, 3:]).max() <= 1e-6 * np.abs(a[:, 3:]).max()
