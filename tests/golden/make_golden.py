@@ -51,12 +51,14 @@ def params_from_json(s):
     return p
 
 
-def _case(name, nf, ncell, order, L, ndirs, seed, rho=0.0, jitter=0.45, masses=None):
+def _case(name, nf, ncell, order, L, ndirs, seed, rho=0.0, jitter=0.45, masses=None, **extra):
     p = api.default_params(nflavors=nf, shape_order=order, ncell=ncell, Lx=L[0], Ly=L[1], Lz=L[2],
                            simulation_type=4, st4_ndens=4.89e32, st4_ndensbar=3.1e32, st4_fluxfac=0.1,
                            st4_fluxfacbar=1.0 / 3.0, st4_theta=0.3, st4_phi=0.2, st4_thetabar=0.1,
                            st4_amplitude=1e-2, direction_generator=1, ndirections=ndirs, seed=seed,
                            rho_in=rho, Ye_in=0.45, cfl_factor=0.5, flavor_cfl_factor=0.4)
+    for k, v in extra.items():
+        api.set_param(p, k, v)
     m = masses or (-0.008596511, 0.0, 0.049487372)
     ev_g = api.EV / api.CLIGHT ** 2
     p.mass1, p.mass2, p.mass3 = m[0] * ev_g, m[1] * ev_g, m[2] * ev_g
@@ -79,6 +81,13 @@ CASES = [
     lambda: _case("nf3_3d", 3, (4, 3, 5), 2, (2.0, 1.5, 2.5), 6, 12, rho=3e9),
     lambda: _case("nf2_cic", 2, (3, 3, 3), 1, (1.5, 1.5, 1.5), 5, 13, rho=1e10),
     lambda: _case("nf3_ngp", 3, (1, 1, 1), 0, (1.0, 1.0, 1.0), 7, 14, rho=1.3e9),
+    # compute_dt's adaptive branch (Evolve.cpp:68-74) with the translation
+    # limit off: dt_flavor = min(speedup dt_stupid, dt_adaptive); the cap
+    # binds at speedup 3, the adaptive potential at 10
+    lambda: _case("nf2_adaptive", 2, (1, 1, 16), 2, (1.0, 1.0, 8.0), 8, 15, rho=2e9, cfl_factor=-1.0,
+                  max_adaptive_speedup=3.0),
+    lambda: _case("nf3_adaptive_3d", 3, (3, 4, 3), 2, (1.5, 2.0, 1.5), 5, 16, rho=2e9, cfl_factor=-1.0,
+                  max_adaptive_speedup=10.0),
 ]
 
 
@@ -118,13 +127,15 @@ def make(name, p, parts):
     return out
 
 
-def main():
+def main(only=None):
     build_oracle.build_ref()
     for c in CASES:
         name, p, parts = c()
+        if only and name not in only:
+            continue
         make(name, p, parts)
         print(name, parts.shape)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

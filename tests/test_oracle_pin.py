@@ -138,3 +138,26 @@ def test_vacuum_potential_theta23_unused():
     nh = 9
     im = [2, 4, 7]
     assert np.allclose(a[nh:][im], -a[:nh][im]) and np.allclose(np.delete(a[nh:], im), np.delete(a[:nh], im))
+
+
+@pytest.mark.parametrize("name,binding", [("nf2_adaptive", "cap"), ("nf3_adaptive_3d", "adaptive")])
+def test_adaptive_fixtures_exercise_the_adaptive_branch(name, binding):
+    """The adaptive-dt fixtures' dt0 comes from Evolve.cpp:68-74: at
+    speedup 3 the cap (3 dt_stupid) binds, at 10 the adaptive potential;
+    either differs from the plain dt_stupid (speedup 0)."""
+    path = [g for g in GOLDEN if g.endswith("golden_%s.npz" % name)][0]
+    p, d = load_golden(path)
+    o = Oracle(p)
+    dt0 = float(d["dt0"])
+    vmax = float(d["vvac_max"])
+    s = p.max_adaptive_speedup
+    p.max_adaptive_speedup = 0.0
+    plain, _ = Oracle(p).compute_dt(d["mesh0"], vmax)
+    p.max_adaptive_speedup = 1e30
+    uncapped, _ = Oracle(p).compute_dt(d["mesh0"], vmax)
+    assert p.cfl_factor < 0 and abs(dt0 - plain) > 0.5 * plain
+    if binding == "cap":
+        assert abs(dt0 - s * plain) <= 1e-13 * dt0 and uncapped > dt0
+    else:
+        assert abs(dt0 - uncapped) <= 1e-13 * dt0 and uncapped < s * plain
+    assert o.compute_dt(d["mesh0"], vmax)[0] == pytest.approx(dt0, rel=1e-13)
