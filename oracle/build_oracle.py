@@ -2,6 +2,8 @@
 
 Outputs:
   oracle/_build/libemu_oracle.so   the C restatement (oracle/emu_oracle.c)
+  oracle/_ref/libemurefinit.so     the reference's direction-set and Minerbo
+                                   helpers (FlavoredNeutrinoContainerInit.cpp)
   oracle/_ref/gen<N>/Source/generated_files/*   the reference generator's output
   oracle/_ref/libemuref<N>.so      the reference's generated kernel bodies,
                                    compiled inside oracle/ref_harness.cpp
@@ -80,10 +82,42 @@ def build_ref(force=False):
     return outs
 
 
+def build_ref_init(force=False):
+    """oracle/_ref/libemurefinit.so: the helper functions at the top of the
+    reference's Source/FlavoredNeutrinoContainerInit.cpp (every line before
+    the FlavoredNeutrinoContainer constructor: uniform_sphere_xyz,
+    minerbo_Z, minerbo_closure, ...), unmodified except that their two
+    #include lines give way to oracle/shim/ref_init_shim.h, followed by
+    oracle/ref_init_api.inc.  None when neither the reference tree nor a
+    prebuilt library exists."""
+    out = os.path.join(REF_OUT, "libemurefinit.so")
+    src = os.path.join(REF_ROOT, "Source", "FlavoredNeutrinoContainerInit.cpp")
+    if not os.path.exists(src):
+        return out if os.path.exists(out) else None
+    api = os.path.join(HERE, "ref_init_api.inc")
+    shim = os.path.join(HERE, "shim", "ref_init_shim.h")
+    if not force and _newer(out, [src, api, shim]):
+        return out
+    lines = open(src).read().splitlines()
+    end = next(i for i, l in enumerate(lines) if l.startswith("FlavoredNeutrinoContainer::"))
+    body = ["// (shim) " + l if l.lstrip().startswith("#include \"") else l for l in lines[:end]]
+    os.makedirs(REF_OUT, exist_ok=True)
+    tu = os.path.join(REF_OUT, "ref_init_tu.cpp")
+    with open(tu, "w") as f:
+        f.write('#include "ref_init_shim.h"\n')
+        f.write('#line 1 "%s"\n' % src)
+        f.write("\n".join(body) + "\n")
+        f.write('#include "ref_init_api.inc"\n')
+    subprocess.check_call(["g++", "-std=c++17"] + CFLAGS + ["-I", os.path.join(HERE, "shim"), "-I", HERE, tu,
+                           "-o", out])
+    return out
+
+
 def build_all(force=False):
     a = build_oracle(force)
     b = build_ref(force)
-    return [a] + b
+    c = build_ref_init(force)
+    return [a] + b + ([c] if c else [])
 
 
 if __name__ == "__main__":

@@ -3,6 +3,8 @@
 Oracle(...)      oracle/_build/libemu_oracle.so  (C restatement, emu_oracle.c)
 RefHarness(nf)   oracle/_ref/libemuref<nf>.so    (the reference's generated
                                                  kernel bodies, ref_harness.cpp)
+RefInit()        oracle/_ref/libemurefinit.so    (the reference's direction-set
+                                                 and Minerbo helpers)
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU legs use this module.
 """
@@ -214,3 +216,37 @@ class RefHarness(_Base):
 
 def have_ref(nf):
     return os.path.exists(REF_LIB % nf)
+
+
+REF_INIT_LIB = os.path.join(HERE, "_ref", "libemurefinit.so")
+
+
+class RefInit:
+    """The reference's initial-condition helpers (uniform_sphere_xyz,
+    minerbo_Z, minerbo_closure of FlavoredNeutrinoContainerInit.cpp),
+    compiled where they lie into oracle/_ref/libemurefinit.so."""
+
+    def __init__(self):
+        self.lib = ctypes.CDLL(REF_INIT_LIB)
+        self.lib.refinit_uniform_sphere_xyz.argtypes = [ctypes.c_int, _D, ctypes.c_int]
+        self.lib.refinit_uniform_sphere_xyz.restype = ctypes.c_int
+        self.lib.refinit_minerbo_Z.argtypes = [ctypes.c_double]
+        self.lib.refinit_minerbo_Z.restype = ctypes.c_double
+        self.lib.refinit_minerbo_closure.argtypes = [ctypes.c_double, ctypes.c_double]
+        self.lib.refinit_minerbo_closure.restype = ctypes.c_double
+
+    def uniform_sphere_xyz(self, nphi):
+        n = self.lib.refinit_uniform_sphere_xyz(nphi, ctypes.cast(None, _D), 0)
+        out = np.zeros((n, 3))
+        self.lib.refinit_uniform_sphere_xyz(nphi, _ptr(out), n)
+        return out
+
+    def minerbo_Z(self, fluxfac):
+        return self.lib.refinit_minerbo_Z(fluxfac)
+
+    def minerbo_closure(self, Z, mu):
+        return self.lib.refinit_minerbo_closure(Z, mu)
+
+
+def have_ref_init():
+    return os.path.exists(REF_INIT_LIB)

@@ -19,6 +19,7 @@ def _built():
     from oracle import build_oracle
     build_oracle.build_oracle()
     build_oracle.build_ref()
+    build_oracle.build_ref_init()
     from emu_b200 import build
     if os.path.exists("/usr/local/cuda/bin/nvcc") or not os.path.exists(build.LIB):
         build.build()
