@@ -389,7 +389,7 @@ int step_generic(emu_context* ctx, double dt)
 
 // deposit: the last stage of the step just taken made no deposit; the
 // gather deposits the new state (cell-sorted) into the next step's first
-// mesh instead (mesh[0] / qmesh[0], zeroed by the step)
+// mesh instead (mesh[0] / qmesh[0], zeroed here first)
 int resort(emu_context* ctx, bool deposit = false)
 {
     DevState& src = ctx->S[ctx->cur];
@@ -399,6 +399,12 @@ int resort(emu_context* ctx, bool deposit = false)
     int r;
     if ((r = sort_perm(ctx, src.n))) return r;
     if (deposit) {
+        // The target is zeroed here, not only by the step before: when the
+        // run has already ended (the step was a no-op), the gather deposits
+        // the unchanged state again, and it must replace the mesh, not add
+        // to it.
+        if (ctx->mixed) CU(cudaMemsetAsync(ctx->qmesh[0], 0, sizeof(long long) * mesh_elems(ctx), ctx->stream));
+        else CU(cudaMemsetAsync(ctx->mesh[0], 0, sizeof(double) * mesh_elems(ctx), ctx->stream));
         emu::launch_gather_deposit(ctx->nf, ctx->mixed, ctx->P, src, dst, ctx->idx2, ctx->mesh[0], ctx->qmesh[0],
                                    ctx->stream);
         if (ctx->mixed) r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[0], true, ctx->stream);
@@ -463,6 +469,10 @@ int emu_ctx::step_device(emu_context* ctx, bool last_stage_deposit)
         cudaError_t e = emu::launch_rk4_step_coop(ctx->nf, ctx->P, ctx->S[ctx->cur], m, mesh_elems(ctx), ctx->ctl,
                                                   emu::DT_ADVANCE, ctx->stream);
         if (e != cudaSuccess) return fail(ctx, EMU_ERR_CUDA, std::string("cooperative step: ") + cudaGetErrorString(e));
+    } else if (ctx->local) {
+        // ranks of a local group rendezvous on the host at every deposit:
+        // the stages are launched one by one
+        if ((r = enqueue_step_body(ctx, ctx->stream, last_stage_deposit))) return r;
     } else {
         const int c = ctx->cur, v = last_stage_deposit ? 0 : 1;
         // the graph holds its kernels' arguments by value: re-capture when
@@ -541,7 +551,7 @@ int emu_ctx::load_from_aos(emu_context* ctx, int64_t n, double pupt_min, const d
     // (step graphs re-capture themselves when P or S differ from their capture)
     // fused == 2: one cooperative launch per step when the grid fits
     // (a sharded run reduces every deposit between stages: per-stage kernels)
-    ctx->coop = !ctx->mixed && !ctx->comm && ctx->prm.fused == 2 && rk4_fused(ctx) &&
+    ctx->coop = !ctx->mixed && !ctx->comm && !ctx->local && ctx->prm.fused == 2 && rk4_fused(ctx) &&
                 emu::coop_step_fits(ctx->nf, ctx->P, n);
     ctx->loaded = true;
     ctx->adj_valid = false;
@@ -615,7 +625,7 @@ int emu_create(const emu_params* p, emu_context** out)
         for (int i = 0; i < 2 && !r; i++)
             if (emu_ctx::dev_malloc(&ctx->qmesh[i], sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
         if (!r && emu_ctx::dev_malloc(&ctx->qfull, sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
-        if (!r && emu_ctx::dev_malloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * 4 * ctx->NH) != cudaSuccess)
+        if (!r && emu_ctx::dev_malloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * (ctx->nf == 3 ? emu::Comb<3>::NG : emu::Comb<2>::NG)) != cudaSuccess)
             r = EMU_ERR_NOMEM;
     } else {
         for (int i = 0; i < 4 && !r; i++)

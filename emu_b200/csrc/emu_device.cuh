@@ -328,6 +328,67 @@ __device__ __forceinline__ unsigned long long f32x2(float a, float b)
     return r;
 }
 
+// d = a * b + c on two FP32 lanes at once
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ float lo32(unsigned long long a)
+{
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+    return lo;
+}
+__device__ __forceinline__ float hi32(unsigned long long a)
+{
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a));
+    return hi;
+}
+
+// Combined self-interaction layout of the mixed path's step meshes and of its
+// FP32 potential mesh: per cell four blocks d (weights 1, v_x, v_y, v_z) of
+// NV values each, q = d * NV + j.  Two flavors: the NF^2 combinations c_e =
+// fN_nu,e - s_e fN_nubar,e (s_e = -1 for imaginary components: the
+// potential's sign rule), NV = 4.  Three flavors: only the traceless part,
+// which is all the commutator sees (the trace commutes with rho): NV = 8,
+// j = (c_00 - tr/3, c_11 - tr/3, c_01 re, im, c_02 re, im, c_12 re, im) with
+// tr = c_00 + c_11 + c_22; c_22 - tr/3 = -(j0 + j1).  32 values per cell: a
+// deposit record stream is exactly one warp, and a cell is eight 16-byte
+// loads.
+template <int NF>
+struct Comb {
+    static constexpr bool TRACELESS = NF == 3;
+    static constexpr int NV = TRACELESS ? 8 : NF * NF;
+    static constexpr int NG = 4 * NV;
+    // values of one particle (or one cell) from its NF^2 combinations c
+    template <class R>
+    __host__ __device__ static void values(const R* c, R* v)
+    {
+        if constexpr (TRACELESS) {
+            const R t3 = (c[0] + c[5] + c[8]) * (R)(1.0 / 3.0);
+            v[0] = c[0] - t3;
+            v[1] = c[5] - t3;
+            v[2] = c[1]; v[3] = c[2]; v[4] = c[3]; v[5] = c[4]; v[6] = c[6]; v[7] = c[7];
+        } else {
+            for (int e = 0; e < NV; e++) v[e] = c[e];
+        }
+    }
+    // the Hermitian components (upper triangle, Re/Im) from the values
+    template <class R>
+    __host__ __device__ static void hermitian(const R* v, R* h)
+    {
+        if constexpr (TRACELESS) {
+            h[0] = v[0]; h[5] = v[1]; h[8] = -(v[0] + v[1]);
+            h[1] = v[2]; h[2] = v[3]; h[3] = v[4]; h[4] = v[5]; h[6] = v[6]; h[7] = v[7];
+        } else {
+            for (int e = 0; e < NV; e++) h[e] = v[e];
+        }
+    }
+};
+
 template <class R, int S, int SP>
 struct RunAcc {
     R a[S];
@@ -360,6 +421,35 @@ struct RunAcc<float, S, SP> {
 #pragma unroll
         for (int k = 0; k < NP; k++)
             asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(a[k]) : "l"(f32x2(w[2 * k], w[2 * k + 1])), "l"(qq));
+    }
+    // the same with the record's weights (16-byte aligned, zero padded to
+    // SP) read as 8-byte pairs straight into the packed FMA's operands
+    __device__ __forceinline__ void add_rec(const float* r, float q)
+    {
+        const unsigned long long qq = f32x2(q, q);
+        const ulonglong2* w2 = reinterpret_cast<const ulonglong2*>(r);
+#pragma unroll
+        for (int k = 0; k < NP; k += 2) {
+            const ulonglong2 w = w2[k / 2];
+            a[k] = fma2(w.x, qq, a[k]);
+            if (k + 1 < NP) a[k + 1] = fma2(w.y, qq, a[k + 1]);
+        }
+    }
+    // two accumulators fed by one read of the weights
+    __device__ __forceinline__ static void add_rec2(RunAcc& x, RunAcc& y, const float* r, float qx, float qy)
+    {
+        const unsigned long long qqx = f32x2(qx, qx), qqy = f32x2(qy, qy);
+        const ulonglong2* w2 = reinterpret_cast<const ulonglong2*>(r);
+#pragma unroll
+        for (int k = 0; k < NP; k += 2) {
+            const ulonglong2 w = w2[k / 2];
+            x.a[k] = fma2(w.x, qqx, x.a[k]);
+            y.a[k] = fma2(w.x, qqy, y.a[k]);
+            if (k + 1 < NP) {
+                x.a[k + 1] = fma2(w.y, qqx, x.a[k + 1]);
+                y.a[k + 1] = fma2(w.y, qqy, y.a[k + 1]);
+            }
+        }
     }
     __device__ __forceinline__ float get(int k) const
     {
@@ -431,36 +521,37 @@ __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, 
         const float b = r[boff];
         const float qv0 = dir0 == 0 ? b : b * r[voff0];
         const float qv1 = b * r[voff1];
-        float w[SP];
-        load_weights<float, SP>(r, w);
-        acc0.add(w, qv0);
-        acc1.add(w, qv1);
+        RunAcc<float, S, SP>::add_rec2(acc0, acc1, r, qv0, qv1);
     }
     if (cur >= 0) flush(cur);
 }
 
-// Combined deposit of the mixed path (FP32 records): per cell the 4 NF^2
-// self-interaction combinations G[d][e] = sum w v_d (fN_nu,e - s_e fN_nubar,e)
-// (v_0 = 1; s_e = -1 for imaginary components: the sign rule of the
-// potential), which is all a stage's interpolation reads.  Records hold the
-// NF^2 combinations c_e; thread q = (d, e) of NSTREAM = BLOCK / (4 NF^2)
-// record streams sums its runs and adds them to mesh[cell * 4 NF^2 + q].
+// Combined deposit of the mixed path (FP32 records): per cell the Comb<NF>
+// values G[d][j] = sum w v_d c_j (v_0 = 1), which is all a stage's
+// interpolation reads.  Records hold the particle's NV values c_j; thread
+// q = (d, j) of NSTREAM = BLOCK / NG record streams sums its runs and adds
+// them to mesh[cell * NG + q].  Three flavors: NG = 32, each stream is one
+// warp (no divergence between streams).  The weights are read as 8-byte
+// pairs straight into the packed FMA's operands.
 template <int NF, int BLOCK, int NTILE, class SWt, class T, class Conv>
 __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, const int* skey, const float* srec,
                                                   int ntile, Conv conv)
 {
     using TR = TileRec<NF, SWt, float>;
-    constexpr int NH = NF * NF, NS = 2 * NH, NG = 4 * NH, RW = TR::RW, SP = TR::SP, S = TR::S;
+    using C = Comb<NF>;
+    constexpr int NS = 2 * NF * NF, NV = C::NV, NG = C::NG, RW = TR::RW, SP = TR::SP, S = TR::S;
+    constexpr int NP = (S + 1) / 2;   // weight pairs
     constexpr int NSTREAM = BLOCK / NG;
     static_assert(NSTREAM >= 1, "one stream of components");
+    static_assert(2 * NP <= SP, "padded weights");
     constexpr int CH = (NTILE + NSTREAM - 1) / NSTREAM;
     const int q = threadIdx.x % NG;
     const int stream = threadIdx.x / NG;
     if (stream >= NSTREAM) return;   // no block-wide barrier follows inside
-    const int d = q / NH, e = q % NH;
-    const int coff = SP + e;
+    const int d = q / NV, j = q % NV;
+    const int coff = SP + j;
     const int voff = SP + NS + (d > 0 ? d - 1 : 0);
-    RunAcc<float, S, SP> acc;
+    unsigned long long acc[NP];
     auto flush = [&](int key) {
         const int bx = key % P.n[0];
         const int by = (key / P.n[0]) % P.n[1];
@@ -472,27 +563,35 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
 #pragma unroll
                 for (int ii = 0; ii < SWt::MX; ii++) {
                     if (!SWt::on(P, ii, jj, kk)) continue;
-                    const T v = conv(acc.get((kk * SWt::MY + jj) * SWt::MX + ii), 0);
-                    if (v != (T)0) atomic_add_mesh(&mesh[cell_of(P, bx, by, bz, ii, jj, kk) * NG + q], v);
+                    const int k = (kk * SWt::MY + jj) * SWt::MX + ii;
+                    const float a = (k & 1) ? hi32(acc[k / 2]) : lo32(acc[k / 2]);
+                    atomic_add_mesh(&mesh[cell_of(P, bx, by, bz, ii, jj, kk) * NG + q], conv(a, 0));
                 }
     };
     const int i1 = min((stream + 1) * CH, ntile);
     int cur = -1;
-    acc.zero();
+#pragma unroll
+    for (int k = 0; k < NP; k++) acc[k] = 0ull;
     for (int i = stream * CH; i < i1; i++) {
         const int key = skey[i];
         if (key != cur) {
             if (cur >= 0) flush(cur);
-            acc.zero();
+#pragma unroll
+            for (int k = 0; k < NP; k++) acc[k] = 0ull;
             cur = key;
         }
         if (key < 0) continue;
         const float* r = srec + i * RW;
         const float b = r[coff];
         const float qv = d == 0 ? b : b * r[voff];
-        float w[SP];
-        load_weights<float, SP>(r, w);
-        acc.add(w, qv);
+        const unsigned long long qq = f32x2(qv, qv);
+        const ulonglong2* w2 = reinterpret_cast<const ulonglong2*>(r);
+#pragma unroll
+        for (int k = 0; k < NP; k += 2) {
+            const ulonglong2 w = w2[k / 2];
+            acc[k] = fma2(w.x, qq, acc[k]);
+            if (k + 1 < NP) acc[k + 1] = fma2(w.y, qq, acc[k + 1]);
+        }
     }
     if (cur >= 0) flush(cur);
 }
@@ -538,9 +637,13 @@ __device__ __forceinline__ void tile_deposit(const DevParams& P, T* mesh, const 
         const R* r = srec + i * RW;
         const R b = r[boff];
         const R qv = dir == 0 ? b : b * r[voff];
-        R w[SP];
-        load_weights<R, SP>(r, w);
-        acc.add(w, qv);
+        if constexpr (sizeof(R) == 4) {
+            acc.add_rec(r, qv);
+        } else {
+            R w[SP];
+            load_weights<R, SP>(r, w);
+            acc.add(w, qv);
+        }
     };
     const int i1 = min((stream + 1) * CH, ntile);
     int cur = -1;

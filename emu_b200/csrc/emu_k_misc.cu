@@ -147,7 +147,7 @@ static unsigned reduce_grid(long long ncells)
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
                            StepCtl* ctl, bool comb, cudaStream_t st)
 {
-    EMU_NF_DISPATCH(nf, (launch_pdl(k_finalize_mixed<NFv>, reduce_grid(P.ncells * 4 * NFv * NFv), kBlock, 0, st, P,
+    EMU_NF_DISPATCH(nf, (launch_pdl(k_finalize_mixed<NFv>, reduce_grid(P.ncells * Comb<NFv>::NG), kBlock, 0, st, P,
                                     qread, qzero, gmesh, ctl, comb ? 1 : 0)));
 }
 
@@ -158,7 +158,7 @@ void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int
 
 void launch_full_to_comb(int nf, const DevParams& P, const long long* qfull, long long* qcomb, cudaStream_t st)
 {
-    EMU_NF_DISPATCH(nf, (k_full_to_comb<NFv><<<reduce_grid(P.ncells * 4 * NFv * NFv), kBlock, 0, st>>>(P, qfull,
+    EMU_NF_DISPATCH(nf, (k_full_to_comb<NFv><<<reduce_grid(P.ncells * 4), kBlock, 0, st>>>(P, qfull,
                                                                                                         qcomb)));
 }
 

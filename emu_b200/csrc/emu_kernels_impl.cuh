@@ -391,14 +391,17 @@ struct QuantConvG {
     const DevParams& P;
     __device__ long long operator()(float a, int) const { return __float2ll_rn(a * (float)P.g_scale); }
 };
-// the NF^2 self-interaction combinations of a particle's f N (nu minus nubar,
-// nu plus nubar for imaginary components: the potential's sign rule)
+// the Comb<NF> values of a particle's f N: the NF^2 self-interaction
+// combinations (nu minus nubar, nu plus nubar for imaginary components: the
+// potential's sign rule), traceless for three flavors
 template <int NF>
-__device__ __forceinline__ void combine_species(const float* fN, float* c)
+__device__ __forceinline__ void combine_species(const float* fN, float* v)
 {
     constexpr int NH = NF * NF;
+    float c[NH];
 #pragma unroll
     for (int e = 0; e < NH; e++) c[e] = Herm<NF>::is_im(e) ? fN[e] + fN[NH + e] : fN[e] - fN[NH + e];
+    Comb<NF>::values(c, v);
 }
 
 // Stable rank of the stencil keys held by the first NW warps of the block
@@ -540,7 +543,7 @@ __device__ __forceinline__ int tile_deposit_block(const DevParams& P, T* mesh, b
         }
     }
     if constexpr (COMB) {
-        tile_record<NF, SWt, R, NF * NF>(srec, skey, slot, key, fN, vx, vy, vz, st);
+        tile_record<NF, SWt, R, Comb<NF>::NV>(srec, skey, slot, key, fN, vx, vy, vz, st);
         __syncthreads();
         tile_deposit_comb<NF, kBlock, kBlock, SWt, T>(P, mesh, skey, srec, kBlock, conv);
     } else {
@@ -1152,50 +1155,66 @@ __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const lo
                                                            StepCtl* ctl, int comb)
 {
     using H = Herm<NF>;
-    constexpr int NH = NF * NF, ND = 8 * NH, NG = 4 * NH;
+    using C = Comb<NF>;
+    constexpr int NH = NF * NF, ND = 8 * NH, NV = C::NV, NG = C::NG;
     grid_dep_wait();   // the previous stage's deposit is complete
     grid_dep_launch();
     if (ctl->done) return;
     zero_slice(qzero, qzero ? P.ncells * ND : 0);
     const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long total = P.ncells * NG;
     if (comb) {
-        // a combined mesh holds G itself
+        // a combined mesh holds the values of G itself
+        const long long total = P.ncells * NG;
         const double f = P.sqrt2GF_inv_vol * P.g_unscale;
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
             g[i] = (float)((double)q[i] * f);
         return;
     }
+    // a full mesh (8 NF^2 per cell, a scale per species): one thread per
+    // (cell, d)
+    const long long total = P.ncells * 4;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        const long long c = i / NG;
-        const int k = (int)(i - c * NG);
-        const int d = k / NH, e = k - d * NH;
-        const long long* m = q + c * ND;
-        const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
-        const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
-        const double comb = H::is_im(e) ? a + b : a - b;
-        g[i] = (float)(P.sqrt2GF_inv_vol * comb);
+        const long long cidx = i / 4;
+        const int d = (int)(i - cidx * 4);
+        const long long* m = q + cidx * ND;
+        double c[NH], v[NV];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
+            const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
+            c[e] = P.sqrt2GF_inv_vol * (H::is_im(e) ? a + b : a - b);
+        }
+        C::values(c, v);
+#pragma unroll
+        for (int j = 0; j < NV; j++) g[cidx * NG + d * NV + j] = (float)v[j];
     }
 }
 
 // full int64 mesh (8 NF^2 per cell, a scale per species) -> the combined
-// self-interaction layout of the step meshes (4 NF^2 per cell, one scale)
+// layout of the step meshes (Comb<NF>: 4 NV per cell, one scale)
 template <int NF>
 __global__ void __launch_bounds__(kBlock) k_full_to_comb(DevParams P, const long long* __restrict__ q,
                                                          long long* __restrict__ out)
 {
     using H = Herm<NF>;
-    constexpr int NH = NF * NF, ND = 8 * NH, NG = 4 * NH;
+    using C = Comb<NF>;
+    constexpr int NH = NF * NF, ND = 8 * NH, NV = C::NV, NG = C::NG;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long total = P.ncells * NG;
+    const long long total = P.ncells * 4;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        const long long c = i / NG;
-        const int k = (int)(i - c * NG);
-        const int d = k / NH, e = k - d * NH;
-        const long long* m = q + c * ND;
-        const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
-        const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
-        out[i] = __double2ll_rn((H::is_im(e) ? a + b : a - b) * P.g_scale);
+        const long long cidx = i / 4;
+        const int d = (int)(i - cidx * 4);
+        const long long* m = q + cidx * ND;
+        double c[NH], v[NV];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            const double a = (double)m[2 * d * NH + e] * P.q_unscale[0];
+            const double b = (double)m[(2 * d + 1) * NH + e] * P.q_unscale[1];
+            c[e] = H::is_im(e) ? a + b : a - b;
+        }
+        C::values(c, v);
+#pragma unroll
+        for (int j = 0; j < NV; j++) out[cidx * NG + d * NV + j] = __double2ll_rn(v[j] * P.g_scale);
     }
 }
 
@@ -1225,32 +1244,49 @@ __global__ void __launch_bounds__(kBlock) k_deposit_q(DevParams P, DevState S, c
     tile_deposit_block<NF, SWt, float>(P, mesh, active, st, fN, vx, vy, vz, QuantConv{P}, true);
 }
 
-// FP32 self-interaction potential from the finalized mesh: H_SI,e (nu); the
-// nubar potential is sgn_e * H_SI,e (generate_code.py:317-355)
+// FP32 self-interaction potential from the finalized mesh: H_SI,e (nu; the
+// traceless part for three flavors); the nubar potential is sgn_e * H_SI,e
+// (generate_code.py:317-355).  Per stencil cell the values come as 8-byte
+// pairs (j, j+1) straight from 16-byte loads into Blackwell's packed FP32
+// FMA: u = G_0 - vx G_x - vy G_y - vz G_z, then H += w u (per component the
+// same FMAs, in the same order, as one component at a time).
 template <int NF, class SWt>
 __device__ __forceinline__ void potential_si32(const DevParams& P, const float* __restrict__ g, const Stencil<float>& st,
                                                float vx, float vy, float vz, float* hs)
 {
-    constexpr int NH = NF * NF;
+    using C = Comb<NF>;
+    constexpr int NV = C::NV, NG = C::NG, NP = NV / 2;
+    static_assert(NV % 4 == 0, "a block of values is whole 16-byte loads");
+    unsigned long long h2[NP];
 #pragma unroll
-    for (int e = 0; e < NH; e++) hs[e] = 0.f;
+    for (int k = 0; k < NP; k++) h2[k] = 0ull;
+    const unsigned long long nvx = f32x2(-vx, -vx), nvy = f32x2(-vy, -vy), nvz = f32x2(-vz, -vz);
     STENCIL_LOOP(SWt, {
         const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
-        // the cell's 4*NH potentials, 16-byte vector loads (cell stride 64 or 144 bytes)
-        const float4* __restrict__ m4 = reinterpret_cast<const float4*>(g + cell * 4 * NH);
-        float m[4 * NH];
+        // the cell's NG values (64 or 128 bytes) as 16-byte loads of two pairs
+        const ulonglong2* __restrict__ m4 = reinterpret_cast<const ulonglong2*>(g + cell * NG);
+        unsigned long long m[NG / 2];
 #pragma unroll
-        for (int k = 0; k < NH; k++) {
-            const float4 v = __ldg(m4 + k);
-            m[4 * k] = v.x; m[4 * k + 1] = v.y; m[4 * k + 2] = v.z; m[4 * k + 3] = v.w;
+        for (int k = 0; k < NG / 4; k++) {
+            const ulonglong2 v = __ldg(m4 + k);
+            m[2 * k] = v.x;
+            m[2 * k + 1] = v.y;
         }
         const float w = st.wx[ii] * st.wy[jj] * st.wz[kk];
+        const unsigned long long ww = f32x2(w, w);
 #pragma unroll
-        for (int e = 0; e < NH; e++) {
-            const float v = m[e] - m[NH + e] * vx - m[2 * NH + e] * vy - m[3 * NH + e] * vz;
-            hs[e] = fmaf(w, v, hs[e]);
+        for (int k = 0; k < NP; k++) {
+            unsigned long long u = m[k];
+            u = fma2(m[NP + k], nvx, u);
+            u = fma2(m[2 * NP + k], nvy, u);
+            u = fma2(m[3 * NP + k], nvz, u);
+            h2[k] = fma2(u, ww, h2[k]);
         }
     })
+    float v[NV];
+#pragma unroll
+    for (int j = 0; j < NV; j++) v[j] = (j & 1) ? hi32(h2[j / 2]) : lo32(h2[j / 2]);
+    C::hermitian(v, hs);
 }
 
 // dynamic shared memory of a mixed stage: the deposit tile, or the staged
@@ -1378,16 +1414,19 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 ksa[c] = s > 1 ? ks32p[c * cap + p] : 0.f;
             }
         }
-        // FP32 self-interaction part, trace removed (it commutes)
+        // FP32 self-interaction part, trace removed (it commutes; three
+        // flavors: the combined mesh holds only the traceless part)
         float hs[NH];
         potential_si32<NF, SWt>(P, gmesh, st, vx, vy, vz, hs);
-        float tr = 0.f;
+        if constexpr (!Comb<NF>::TRACELESS) {
+            float tr = 0.f;
 #pragma unroll
-        for (int i = 0; i < NF; i++) tr += hs[H::re(i, i)];
-        tr *= (1.0f / NF);
+            for (int i = 0; i < NF; i++) tr += hs[H::re(i, i)];
+            tr *= (1.0f / NF);
 #pragma unroll
-        for (int e = 0; e < NH; e++)
-            if (H::is_diag(e)) hs[e] -= tr;
+            for (int e = 0; e < NH; e++)
+                if (H::is_diag(e)) hs[e] -= tr;
+        }
         const float ih = (float)P.inv_hbar;
         const double mat = P.sqrt2GF_inv_vol * P.matter;
         const double aw = s > 1 ? dt * kRK4A[s - 1] : 0.0;
@@ -1506,7 +1545,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         } else {
             // M_2, M_3 and the next step's M_1: only the combinations the
             // stages interpolate
-            float cN[NH];
+            float cN[Comb<NF>::NV];
             combine_species<NF>(fN, cN);
             const int sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(
                 P, qout, live, st, cN, vx, vy, vz, QuantConvG{P}, s == 4, given);
@@ -1687,7 +1726,7 @@ __global__ void __launch_bounds__(kBlock) k_gather_deposit(DevParams P, DevState
     }
     if constexpr (MIXED) {
         // the next step's first mesh: the combined layout
-        float cN[NH];
+        float cN[Comb<NF>::NV];
         combine_species<NF>(fN, cN);
         tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(P, qmesh, active, st, cN, vx, vy, vz,
                                                                         QuantConvG{P});

@@ -53,7 +53,10 @@ def test_one_step_vs_golden(path, integ):
     k = {"rk4_coop": 4, "rk4_fused": 4, "rk4_unfused": 4, "fe": 0, "trapezoid": 2, "ssprk3": 3}[integ]
     with _ctx(p, resort_interval=0, **kw) as c:
         c.load_particles(d["parts"])
-        code, bad = c.step(float(d["dt0"]))
+        # (forward Euler with the 3D adaptive fixture's large dt leaves a
+        # flavor-vector length error that Renormalize reports, as the
+        # reference's arithmetic does)
+        code, bad = c.step(float(d["dt0"]), raise_on_error=False)
         assert code == int(d["status_%d" % k])
         assert colwise_rel(c.get_particles(), d["step_%d" % k]) < TOL
         assert mesh_rel(c.get_mesh(), d["mesh_%d" % k], nc) < TOL
