@@ -135,6 +135,9 @@ SIGNATURES = {
     "emu_init_particles_device": (ctypes.c_int, [ctypes.c_void_p]),
     "emu_comm_id": (ctypes.c_int, [ctypes.c_char_p]),
     "emu_attach_comm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "emu_local_group_create": (ctypes.c_int, [ctypes.c_int, _P(ctypes.c_void_p)]),
+    "emu_attach_local": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "emu_local_group_destroy": (None, [ctypes.c_void_p]),
     "emu_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D,
                                            _P(EmuRunInfo)]),
     "emu_adjoint_objective": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
@@ -146,6 +149,23 @@ SIGNATURES = {
 
 
 COMM_ID_BYTES = 128
+
+
+class LocalGroup:
+    """Ranks of the sharded schedule that are contexts of this process
+    (emu_local_group_create): each rank's context is driven from its own
+    thread.  Destroy (close) after every member context is closed."""
+
+    def __init__(self, nranks):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self.lib.emu_local_group_create(int(nranks), ctypes.byref(h)), None, "emu_local_group_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.emu_local_group_destroy(self.h)
+            self.h = None
 
 
 def comm_id():
@@ -393,6 +413,10 @@ class Context:
     def init_particles_device(self):
         """InitParticles on the device, loaded into this context"""
         self._ck(self.lib.emu_init_particles_device(self.h), "emu_init_particles_device")
+
+    def attach_local(self, group, rank):
+        """join rank `rank` of a LocalGroup (before load_particles)"""
+        self._ck(self.lib.emu_attach_local(self.h, group.h, int(rank)), "emu_attach_local")
 
     def attach_comm(self, comm_id, rank, nranks):
         """join a particle-sharding communicator (before load_particles)"""

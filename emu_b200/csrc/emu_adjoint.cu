@@ -1121,7 +1121,7 @@ int check_ready(emu_context* ctx, const char* who)
 {
     if (!ctx->loaded) return fail(ctx, EMU_ERR_STATE, std::string(who) + ": no particles loaded");
     if (ctx->mixed) return fail(ctx, EMU_ERR_ARG, std::string(who) + ": the adjoint is FP64 only");
-    if (ctx->comm) return fail(ctx, EMU_ERR_ARG, std::string(who) + ": the adjoint runs on one GPU");
+    if (ctx->comm || ctx->local) return fail(ctx, EMU_ERR_ARG, std::string(who) + ": the adjoint runs on one GPU");
     if (!(ctx->prm.integration_type == 1 && ctx->prm.rk_type == 4))
         return fail(ctx, EMU_ERR_ARG, std::string(who) + ": the adjoint differentiates RK4 only");
     return EMU_OK;

@@ -14,9 +14,13 @@
 
 #include <dlfcn.h>
 
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 using emu_ctx::check_launch;
 using emu_ctx::fail;
@@ -64,8 +68,120 @@ int nccl_fail(emu_context* ctx, ncclResult_t r, const char* what)
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Ranks that are contexts of one process (emu_local_group_*): the same
+// sharded schedule with the exchange done by the library itself, so that it
+// runs with several ranks on one GPU (NCCL takes one GPU per rank).  Each
+// rank's host thread drives its context on its own stream; a reduction is a
+// host rendezvous of the ranks plus stream-ordered work: every rank copies
+// its contribution into its send buffer and records an event, and after the
+// rendezvous every rank's stream waits for all those events and sums the
+// send buffers in rank order (integer sums exact, FP64 sums in a fixed
+// order), so no kernel waits on another.  A second rendezvous keeps a send
+// buffer from being refilled before every rank has issued its reads.  Step
+// graphs are not used by such ranks (a rendezvous is host work).
+namespace {
+
+struct LocalGroup {
+    int nranks = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    long long gen = 0;
+    int arrived = 0;
+    std::vector<void*> send;            // per rank: mesh-sized device buffer
+    std::vector<cudaEvent_t> ready, done;
+    size_t bytes = 0;
+    double scal[64][8];
+    bool broken = false;
+};
+
+constexpr int kLocalMaxRanks = 64;
+constexpr std::chrono::seconds kRendezvousLimit(120);
+
+// all ranks arrive (false: a rank did not come within the limit, or an
+// earlier rendezvous failed)
+bool rendezvous(LocalGroup& g)
+{
+    std::unique_lock<std::mutex> lk(g.mu);
+    if (g.broken) return false;
+    const long long my = g.gen;
+    if (++g.arrived == g.nranks) {
+        g.arrived = 0;
+        g.gen++;
+        g.cv.notify_all();
+        return true;
+    }
+    if (!g.cv.wait_for(lk, kRendezvousLimit, [&] { return g.gen != my || g.broken; }) || g.broken) {
+        g.broken = true;
+        g.cv.notify_all();
+        return false;
+    }
+    return true;
+}
+
+struct RankPtrs {
+    const void* p[kLocalMaxRanks];
+};
+
+template <class T>
+__global__ void k_sum_ranks(T* __restrict__ out, RankPtrs in, int nranks, long long n)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        T s = static_cast<const T*>(in.p[0])[i];
+        for (int r = 1; r < nranks; r++) s += static_cast<const T*>(in.p[r])[i];
+        out[i] = s;
+    }
+}
+
+int local_reduce_mesh(emu_context* ctx, void* mesh, bool int64, size_t count, cudaStream_t st)
+{
+    LocalGroup& g = *static_cast<LocalGroup*>(ctx->local);
+    const int r = ctx->rank;
+    if (count * 8 > g.bytes) return fail(ctx, EMU_ERR_STATE, "local group: mesh larger than the send buffers");
+    for (int k = 0; k < g.nranks; k++) CU(cudaStreamWaitEvent(st, g.done[k], 0));
+    CU(cudaMemcpyAsync(g.send[r], mesh, count * 8, cudaMemcpyDeviceToDevice, st));
+    CU(cudaEventRecord(g.ready[r], st));
+    if (!rendezvous(g)) return fail(ctx, EMU_ERR_STATE, "local group: a rank did not reach the mesh reduction");
+    RankPtrs ptrs{};
+    for (int k = 0; k < g.nranks; k++) {
+        CU(cudaStreamWaitEvent(st, g.ready[k], 0));
+        ptrs.p[k] = g.send[k];
+    }
+    const unsigned grid = (unsigned)std::min<long long>(((long long)count + 255) / 256, 148 * 8);
+    if (int64) k_sum_ranks<long long><<<grid, 256, 0, st>>>(static_cast<long long*>(mesh), ptrs, g.nranks, count);
+    else k_sum_ranks<double><<<grid, 256, 0, st>>>(static_cast<double*>(mesh), ptrs, g.nranks, count);
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(g.done[r], st));
+    if (!rendezvous(g)) return fail(ctx, EMU_ERR_STATE, "local group: a rank did not finish the mesh reduction");
+    return EMU_OK;
+}
+
+int local_reduce_scalars(emu_context* ctx, double* v, int n, int op)
+{
+    LocalGroup& g = *static_cast<LocalGroup*>(ctx->local);
+    {
+        std::lock_guard<std::mutex> lk(g.mu);
+        for (int i = 0; i < n; i++) g.scal[ctx->rank][i] = v[i];
+    }
+    if (!rendezvous(g)) return fail(ctx, EMU_ERR_STATE, "local group: a rank did not reach a scalar reduction");
+    {
+        std::lock_guard<std::mutex> lk(g.mu);
+        for (int i = 0; i < n; i++) {
+            double a = g.scal[0][i];
+            for (int k = 1; k < g.nranks; k++) a = op ? std::max(a, g.scal[k][i]) : a + g.scal[k][i];
+            v[i] = a;
+        }
+    }
+    if (!rendezvous(g)) return fail(ctx, EMU_ERR_STATE, "local group: a rank did not finish a scalar reduction");
+    return EMU_OK;
+}
+
+}  // namespace
+
 int emu_ctx::reduce_mesh(emu_context* ctx, void* mesh, bool int64, cudaStream_t st)
 {
+    if (ctx->local) return local_reduce_mesh(ctx, mesh, int64, (size_t)ctx->P.ncells * ctx->ND, st);
     if (!ctx->comm) return EMU_OK;
     const size_t count = (size_t)ctx->P.ncells * ctx->ND;
     ncclResult_t r = nccl().AllReduce(mesh, mesh, count, int64 ? ncclInt64 : ncclFloat64, ncclSum,
@@ -76,6 +192,8 @@ int emu_ctx::reduce_mesh(emu_context* ctx, void* mesh, bool int64, cudaStream_t 
 // sum (op 0) or max (op 1) of host scalars over the ranks; synchronous
 int emu_ctx_reduce_scalars(emu_context* ctx, double* v, int n, int op)
 {
+    if (ctx->local) return n > 8 ? fail(ctx, EMU_ERR_ARG, "reduce_scalars: too many values")
+                                 : local_reduce_scalars(ctx, v, n, op);
     if (!ctx->comm) return EMU_OK;
     if (n > 8) return fail(ctx, EMU_ERR_ARG, "reduce_scalars: too many values");
     CU(cudaMemcpyAsync(ctx->red_scratch, v, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
@@ -89,6 +207,7 @@ int emu_ctx_reduce_scalars(emu_context* ctx, double* v, int n, int op)
 
 void emu_ctx_comm_free(emu_context* ctx)
 {
+    ctx->local = nullptr;   // (the group owns its buffers)
     if (ctx->comm) nccl().CommDestroy(static_cast<ncclComm_t>(ctx->comm));
     ctx->comm = nullptr;
     if (ctx->red_scratch) emu_ctx::dev_free(ctx->red_scratch);
@@ -127,6 +246,61 @@ int emu_attach_comm(emu_context* ctx, const char* id, int rank, int nranks)
     ctx->rank = rank;
     ctx->nranks = nranks;
     CU(emu_ctx::dev_malloc(&ctx->red_scratch, 8 * sizeof(double)));
+    return EMU_OK;
+}
+
+int emu_local_group_create(int nranks, void** group)
+{
+    if (!group || nranks < 1 || nranks > kLocalMaxRanks)
+        return fail(nullptr, EMU_ERR_ARG, "emu_local_group_create: bad arguments");
+    auto* g = new LocalGroup();
+    g->nranks = nranks;
+    g->send.assign(nranks, nullptr);
+    g->ready.assign(nranks, nullptr);
+    g->done.assign(nranks, nullptr);
+    for (int k = 0; k < nranks; k++) {
+        if (cudaEventCreateWithFlags(&g->ready[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g->done[k], cudaEventDisableTiming) != cudaSuccess) {
+            emu_local_group_destroy(g);
+            return fail(nullptr, EMU_ERR_CUDA, "emu_local_group_create: event creation failed");
+        }
+    }
+    *group = g;
+    return EMU_OK;
+}
+
+void emu_local_group_destroy(void* group)
+{
+    auto* g = static_cast<LocalGroup*>(group);
+    if (!g) return;
+    cudaDeviceSynchronize();
+    for (int k = 0; k < g->nranks; k++) {
+        if (g->send[k]) emu_ctx::dev_free(g->send[k]);
+        if (g->ready[k]) cudaEventDestroy(g->ready[k]);
+        if (g->done[k]) cudaEventDestroy(g->done[k]);
+    }
+    delete g;
+}
+
+int emu_attach_local(emu_context* ctx, void* group, int rank)
+{
+    auto* g = static_cast<LocalGroup*>(group);
+    if (!ctx || !g || rank < 0 || rank >= g->nranks) return fail(ctx, EMU_ERR_ARG, "emu_attach_local: bad arguments");
+    if (ctx->comm || ctx->local) return fail(ctx, EMU_ERR_STATE, "emu_attach_local: a communicator is already attached");
+    if (ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_attach_local: attach before loading particles");
+    const size_t bytes = (size_t)ctx->P.ncells * ctx->ND * 8;
+    {
+        std::lock_guard<std::mutex> lk(g->mu);
+        if (g->send[rank]) return fail(ctx, EMU_ERR_STATE, "emu_attach_local: rank already attached");
+        if (g->bytes && g->bytes != bytes) return fail(ctx, EMU_ERR_ARG, "emu_attach_local: mesh size differs");
+        g->bytes = bytes;
+        void* b = nullptr;
+        if (emu_ctx::dev_malloc(&b, bytes) != cudaSuccess) return fail(ctx, EMU_ERR_NOMEM, "emu_attach_local");
+        g->send[rank] = b;
+    }
+    ctx->local = g;
+    ctx->rank = rank;
+    ctx->nranks = g->nranks;
     return EMU_OK;
 }
 

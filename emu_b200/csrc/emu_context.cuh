@@ -59,6 +59,7 @@ struct emu_context {
     // particle sharding over ranks (emu_attach_comm): every deposit is summed
     // over the ranks before a stage reads it
     void* comm = nullptr;               // ncclComm_t
+    void* local = nullptr;              // or a LocalGroup: ranks that are contexts of one process
     int rank = 0, nranks = 1;
     double* red_scratch = nullptr;      // device scalars for load-time reductions
     double* stats = nullptr;            // per-block record statistics of a load (device)

@@ -331,6 +331,24 @@ int emu_deposit_noalloc(const emu_params* p, const double* d_records, int64_t n,
 #define EMU_COMM_ID_BYTES 128
 int emu_comm_id(char* id);
 int emu_attach_comm(emu_context* ctx, const char* id, int rank, int nranks);
+/*
+ * The same sharded schedule with ranks that are contexts of one process, on
+ * one GPU or several (no counterpart in the reference): every rank's host
+ * thread drives its own context on its own stream, and the library itself
+ * does the exchange (a host rendezvous of the ranks at every reduction, then
+ * stream-ordered copies and a rank-ordered sum; no kernel waits on another).
+ * Used to run the multi-rank path where one GPU is all there is; step
+ * graphs are not used by such ranks.
+ *   emu_local_group_create: a group of nranks ranks (at most 64).
+ *   emu_attach_local: joins rank `rank` of the group (before
+ *     emu_load_particles); every rank must then make the same calls in the
+ *     same order (loads and steps), each from its own thread.  A rank that
+ *     does not arrive within 120 s fails the others' calls (EMU_ERR_STATE).
+ *   emu_local_group_destroy: after every member context is destroyed.
+ */
+int emu_local_group_create(int nranks, void** group);
+int emu_attach_local(emu_context* ctx, void* group, int rank);
+void emu_local_group_destroy(void* group);
 
 int emu_adjoint_forward(emu_context* ctx, int nsteps, int checkpoint_interval, double start_time, double* dts,
                         emu_run_info* info);
