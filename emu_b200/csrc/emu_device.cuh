@@ -468,7 +468,8 @@ struct RunAcc<float, S, SP> {
 // f N, velocity factors d and d + 2), so that one load of a record's stencil
 // weights and f N serves two run sums per cell; 36 pairs per stream, three
 // streams of records per 128-thread CTA (a component per thread leaves one
-// stream of 72 threads).
+// stream of 72 threads).  (Warp-aligned streams with a second pass for the
+// components beyond 64 measured slower: 12.1 against 10.5 ms per C5 launch.)
 template <int BLOCK, int NTILE, class SWt, class T, class Conv>
 __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, const int* skey, const float* srec,
                                                    int ntile, Conv conv)
@@ -521,7 +522,10 @@ __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, 
         const float b = r[boff];
         const float qv0 = dir0 == 0 ? b : b * r[voff0];
         const float qv1 = b * r[voff1];
-        RunAcc<float, S, SP>::add_rec2(acc0, acc1, r, qv0, qv1);
+        float w[SP];
+        load_weights<float, SP>(r, w);
+        acc0.add(w, qv0);
+        acc1.add(w, qv1);
     }
     if (cur >= 0) flush(cur);
 }
