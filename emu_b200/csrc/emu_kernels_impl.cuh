@@ -1246,59 +1246,118 @@ __global__ void __launch_bounds__(kBlock) k_deposit_q(DevParams P, DevState S, c
 
 // FP32 self-interaction potential from the finalized mesh: H_SI,e (nu; the
 // traceless part for three flavors); the nubar potential is sgn_e * H_SI,e
-// (generate_code.py:317-355).  Per stencil cell the values come as 8-byte
-// pairs (j, j+1) straight from 16-byte loads into Blackwell's packed FP32
-// FMA: u = G_0 - vx G_x - vy G_y - vz G_z, then H += w u (per component the
-// same FMAs, in the same order, as one component at a time).
-template <int NF, class SWt>
-__device__ __forceinline__ void potential_si32(const DevParams& P, const float* __restrict__ g, const Stencil<float>& st,
-                                               float vx, float vy, float vz, float* hs)
+// (generate_code.py:317-355).  Per stencil cell the values come from 16-byte
+// loads as pairs (j, j+1) of Blackwell's packed FP32 FMA:
+// u = G_0 - vx G_x - vy G_y - vz G_z, then H += w u (per component the same
+// FMAs, in the same order, as one component at a time).  cell4(ii, jj, kk, k)
+// returns the k-th 16-byte vector of stencil cell (ii, jj, kk): from the
+// mesh in global memory, or from the CTA's staged neighbourhood.
+template <int NF, class SWt, class Cell4>
+__device__ __forceinline__ void potential_si32_from(const DevParams& P, Cell4 cell4, const Stencil<float>& st,
+                                                    float vx, float vy, float vz, float* hs)
 {
     using C = Comb<NF>;
     constexpr int NV = C::NV, NG = C::NG, NP = NV / 2;
     static_assert(NV % 4 == 0, "a block of values is whole 16-byte loads");
-    unsigned long long h2[NP];
+    float2 h2[NP];
 #pragma unroll
-    for (int k = 0; k < NP; k++) h2[k] = 0ull;
-    const unsigned long long nvx = f32x2(-vx, -vx), nvy = f32x2(-vy, -vy), nvz = f32x2(-vz, -vz);
+    for (int k = 0; k < NP; k++) h2[k] = f2(0.f, 0.f);
+    const float2 nvx = f2(-vx, -vx), nvy = f2(-vy, -vy), nvz = f2(-vz, -vz);
     STENCIL_LOOP(SWt, {
-        const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
-        // the cell's NG values (64 or 128 bytes) as 16-byte loads of two pairs
-        const ulonglong2* __restrict__ m4 = reinterpret_cast<const ulonglong2*>(g + cell * NG);
-        unsigned long long m[NG / 2];
+        float2 m[NG / 2];
 #pragma unroll
         for (int k = 0; k < NG / 4; k++) {
-            const ulonglong2 v = __ldg(m4 + k);
-            m[2 * k] = v.x;
-            m[2 * k + 1] = v.y;
+            const float4 v = cell4(ii, jj, kk, k);
+            m[2 * k] = f2(v.x, v.y);
+            m[2 * k + 1] = f2(v.z, v.w);
         }
         const float w = st.wx[ii] * st.wy[jj] * st.wz[kk];
-        const unsigned long long ww = f32x2(w, w);
+        const float2 ww = f2(w, w);
 #pragma unroll
         for (int k = 0; k < NP; k++) {
-            unsigned long long u = m[k];
-            u = fma2(m[NP + k], nvx, u);
-            u = fma2(m[2 * NP + k], nvy, u);
-            u = fma2(m[3 * NP + k], nvz, u);
-            h2[k] = fma2(u, ww, h2[k]);
+            float2 u = __ffma2_rn(m[NP + k], nvx, m[k]);
+            u = __ffma2_rn(m[2 * NP + k], nvy, u);
+            u = __ffma2_rn(m[3 * NP + k], nvz, u);
+            h2[k] = __ffma2_rn(u, ww, h2[k]);
         }
     })
     float v[NV];
 #pragma unroll
-    for (int j = 0; j < NV; j++) v[j] = (j & 1) ? hi32(h2[j / 2]) : lo32(h2[j / 2]);
+    for (int j = 0; j < NV; j++) v[j] = (j & 1) ? h2[j / 2].y : h2[j / 2].x;
     C::hermitian(v, hs);
+}
+
+template <int NF, class SWt>
+__device__ __forceinline__ void potential_si32(const DevParams& P, const float* __restrict__ g, const Stencil<float>& st,
+                                               float vx, float vy, float vz, float* hs)
+{
+    constexpr int NG = Comb<NF>::NG;
+    potential_si32_from<NF, SWt>(
+        P,
+        [&](int ii, int jj, int kk, int k) {
+            const long long cell = cell_of(P, st.b[0], st.b[1], st.b[2], ii, jj, kk);
+            return __ldg(reinterpret_cast<const float4*>(g + cell * NG) + k);
+        },
+        st, vx, vy, vz, hs);
+}
+
+// The neighbourhood of a CTA's particles for 27-cell stencils: the box of
+// cells their stencils touch, staged in shared memory by bulk copies (the TMA
+// engine, no multicast) of the potential mesh's rows when it holds at most
+// kMeshTileCells cells.  Built from the smallest and largest stencil key of
+// the CTA: every key between them lies in one z plane and in one or two
+// consecutive y rows, so the box is x from the smallest key's x to the
+// largest's (+ nx when the rows differ), y over one or two rows, z one
+// plane, each grown by the stencil's two further cells.  Otherwise (keys
+// spread wider, a mesh smaller than a box) the interpolation reads the mesh
+// in global memory.
+constexpr int kMeshTileCells = 80;
+
+struct MeshBox {
+    int x0, y0, z0;   // first cell of the box (wrapped)
+    int nx, ny, nz;   // its extent; nx = 0: not staged
+};
+
+__device__ __forceinline__ MeshBox mesh_box(const DevParams& P, unsigned kmin, unsigned kmax)
+{
+    MeshBox b{0, 0, 0, 0, 0, 0};
+    if (kmin > kmax) return b;   // no particle
+    const int n0 = P.n[0], n1 = P.n[1];
+    const int xa = (int)(kmin % n0), ya = (int)((kmin / n0) % n1), za = (int)(kmin / (n0 * n1));
+    const int xb = (int)(kmax % n0), yb = (int)((kmax / n0) % n1), zb = (int)(kmax / (n0 * n1));
+    if (za != zb || (yb != ya && yb != ya + 1)) return b;
+    const int lx = (yb == ya ? xb - xa : xb + n0 - xa) + 3;
+    const int ly = yb - ya + 3;
+    if (lx > n0 || ly > n1 || 3 > P.n[2] || lx * ly * 3 > kMeshTileCells) return b;
+    b.x0 = xa; b.y0 = ya; b.z0 = za;
+    b.nx = lx; b.ny = ly; b.nz = 3;
+    return b;
 }
 
 // dynamic shared memory of a mixed stage: the deposit tile, or the staged
 // state slices (f0 FP64, k32 and ksum32 FP32) when those are larger
 template <int NF, int WX, int WY, int WZ>
-constexpr int mixed_stage_smem_bytes()
+__host__ __device__ constexpr bool mixed_mesh_tile()
+{
+    return WX == 3 && WY == 3 && WZ == 3;
+}
+
+template <int NF, int WX, int WY, int WZ>
+__host__ __device__ constexpr int mixed_stage_smem_bytes()
 {
     constexpr int tile = tile_smem_bytes<NF, SW<WX, WY, WZ>, float>();
     using SWt = SW<WX, WY, WZ>;
     constexpr bool preload = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
     constexpr int staged = preload ? 0 : 2 * NF * NF * kBlock * 16 + 7 * kBlock * 8;
-    return tile > staged ? tile : staged;
+    constexpr int area = tile > staged ? tile : staged;
+    // (after the area: the staged mesh neighbourhood of 27-cell stencils)
+    return area + (mixed_mesh_tile<NF, WX, WY, WZ>() ? kMeshTileCells * Comb<NF>::NG * 4 : 0);
+}
+template <int NF, int WX, int WY, int WZ>
+__host__ __device__ constexpr int mixed_mesh_tile_offset()
+{
+    return mixed_stage_smem_bytes<NF, WX, WY, WZ>() -
+           (mixed_mesh_tile<NF, WX, WY, WZ>() ? kMeshTileCells * Comb<NF>::NG * 4 : 0);
 }
 
 template <int NF, int WX, int WY, int WZ>
@@ -1328,6 +1387,13 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     const int t = threadIdx.x;
     extern __shared__ __align__(16) unsigned char tile_smem[];
     __shared__ __align__(8) unsigned long long stage_bar;
+    // 27-cell stencils: the staged mesh neighbourhood (see mesh_box)
+    constexpr bool MTILE = STAGE && mixed_mesh_tile<NF, WX, WY, WZ>();
+    constexpr int NGC = Comb<NF>::NG;
+    __shared__ __align__(8) unsigned long long mesh_bar;
+    __shared__ unsigned key_ext[2][kBlock / 32];
+    __shared__ MeshBox mbox;
+    float* const mtile = reinterpret_cast<float*>(tile_smem + mixed_mesh_tile_offset<NF, WX, WY, WZ>());
     double* const sf0 = reinterpret_cast<double*>(tile_smem);        // [NS][kBlock]
     float* const sk = reinterpret_cast<float*>(sf0 + NS * kBlock);   // [NS][kBlock]
     float* const sks = sk + NS * kBlock;                             // [NS][kBlock]
@@ -1341,6 +1407,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 mbar_init(&stage_bar, 1);
                 mbar_expect_tx(&stage_bar, NS * kBlock * 8 + (s > 1 ? 2 * NS * kBlock * 4 : 0) +
                                                (s == 4 ? 7 * kBlock * 8 : 0));
+                if constexpr (MTILE) mbar_init(&mesh_bar, 1);
             }
             __syncwarp();
             for (int c = t; c < NS; c += 32) bulk_g2s(sf0 + c * kBlock, S.f0 + c * cap + p0, kBlock * 8, &stage_bar);
@@ -1390,6 +1457,17 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         }
         make_stencil<float>(P, x, y, z, st);
     }
+    if constexpr (MTILE) {
+        // the CTA's smallest and largest stencil key
+        const unsigned key = active ? (unsigned)stencil_key(P, st.b) : 0u;
+        const unsigned kmin = __reduce_min_sync(kFull, active ? key : 0xffffffffu);
+        const unsigned kmax = __reduce_max_sync(kFull, key);
+        if ((t & 31) == 0) {
+            key_ext[0][t >> 5] = kmin;
+            key_ext[1][t >> 5] = kmax;
+        }
+        __syncthreads();
+    }
     grid_dep_wait();
     grid_dep_launch();
     bool live = active;   // false: this particle's staged state never arrived
@@ -1399,6 +1477,38 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 const float* src = c < NS ? S.k32 + c * cap + p0 : S.ksum32 + (c - NS) * cap + p0;
                 bulk_g2s(sk + c * kBlock, src, kBlock * 4, &stage_bar);
             }
+    }
+    if constexpr (MTILE) {
+        // the neighbourhood's rows of the potential mesh (written by the
+        // finalize kernel this stage waited for): one or two contiguous x
+        // segments per (y, z) row, one lane per row
+        if (t < 32) {
+            if (t == 0) {
+                unsigned kmin = key_ext[0][0], kmax = key_ext[1][0];
+#pragma unroll
+                for (int w = 1; w < kBlock / 32; w++) {
+                    kmin = min(kmin, key_ext[0][w]);
+                    kmax = max(kmax, key_ext[1][w]);
+                }
+                const MeshBox b = mesh_box(P, kmin, kmax);
+                mbox = b;
+                mbar_expect_tx(&mesh_bar, (unsigned)(b.nx * b.ny * b.nz * NGC * 4));
+            }
+            __syncwarp();
+            const MeshBox b = mbox;
+            const int nrow = b.ny * b.nz;
+            for (int row = t; row < nrow; row += 32) {
+                const int yy = row % b.ny, zz = row / b.ny;
+                const int gy = (b.y0 + yy) % P.n[1], gz = (b.z0 + zz) % P.n[2];
+                const long long grow = ((long long)gz * P.n[1] + gy) * P.n[0];
+                float* dst = mtile + (long long)row * b.nx * NGC;
+                // x from b.x0 over b.nx cells, split where it wraps
+                const int first = min(b.nx, P.n[0] - b.x0);
+                bulk_g2s(dst, gmesh + (grow + b.x0) * NGC, (unsigned)(first * NGC * 4), &mesh_bar);
+                if (first < b.nx)
+                    bulk_g2s(dst + first * NGC, gmesh + grow * NGC, (unsigned)((b.nx - first) * NGC * 4), &mesh_bar);
+            }
+        }
     }
     // compute_dt on the stage-4 mesh (every block has read this step's dt)
     if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
@@ -1417,7 +1527,28 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         // FP32 self-interaction part, trace removed (it commutes; three
         // flavors: the combined mesh holds only the traceless part)
         float hs[NH];
-        potential_si32<NF, SWt>(P, gmesh, st, vx, vy, vz, hs);
+        bool tiled = false;
+        if constexpr (MTILE) {
+            // (the wait also orders mbox, written before the arrival)
+            if (!mbar_wait(&mesh_bar, 0)) {
+                atomicOr(&ctl->status, ST_TIMEOUT);
+                live = false;
+            } else {
+                const MeshBox b = mbox;
+                const int lx = wrapi(st.b[0] - b.x0, P.n[0]), ly = wrapi(st.b[1] - b.y0, P.n[1]),
+                          lz = wrapi(st.b[2] - b.z0, P.n[2]);
+                if (b.nx > 0 && lx + 2 < b.nx && ly + 2 < b.ny && lz + 2 < b.nz) {
+                    tiled = true;
+                    const float4* base =
+                        reinterpret_cast<const float4*>(mtile + ((lz * b.ny + ly) * b.nx + lx) * NGC);
+                    const int sy = b.nx * NGC / 4, sz = b.ny * b.nx * NGC / 4;
+                    potential_si32_from<NF, SWt>(
+                        P, [&](int ii, int jj, int kk, int k) { return base[kk * sz + jj * sy + ii * (NGC / 4) + k]; },
+                        st, vx, vy, vz, hs);
+                }
+            }
+        }
+        if (!tiled) potential_si32<NF, SWt>(P, gmesh, st, vx, vy, vz, hs);
         if constexpr (!Comb<NF>::TRACELESS) {
             float tr = 0.f;
 #pragma unroll
@@ -1529,7 +1660,8 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         // the staged state is consumed (and the copies complete) before the
         // deposit records reuse the area; when the copies do not complete
         // within the bounded wait the CTA deposits nothing
-        const bool drained = __syncthreads_and(t != 0 || mbar_wait(&stage_bar, 0));
+        const bool drained =
+            __syncthreads_and(t != 0 || (mbar_wait(&stage_bar, 0) && (!MTILE || mbar_wait(&mesh_bar, 0))));
         if (!drained) {
             if (t == 0) atomicOr(&ctl->status, ST_TIMEOUT);
             return;
@@ -1955,9 +2087,12 @@ template <int NF>
 void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, const float* gmesh, long long* qout,
                               const long long* qdt, StepCtl* ctl, int dt_mode, cudaStream_t st)
 {
-    EMU_W_DISPATCH(P, (launch_pdl(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock,
-                                  mixed_stage_smem_bytes<NF, WXv, WYv, WZv>(), st, P, S, s, gmesh, qout, qdt, ctl,
-                                  dt_mode)));
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = mixed_stage_smem_bytes<NF, WXv, WYv, WZv>();
+        smem_optin(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, bytes);
+        launch_pdl(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock, bytes, st, P, S, s, gmesh, qout, qdt,
+                   ctl, dt_mode);
+    });
 }
 
 template <int NF>
