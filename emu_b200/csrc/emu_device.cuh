@@ -411,6 +411,22 @@ struct RunAcc<float, S, SP> {
             if (k + 1 < NP) a[k + 1] = __ffma2_rn(f2(w.z, w.w), qq, a[k + 1]);
         }
     }
+    // two accumulators fed by one read of the weights
+    __device__ __forceinline__ static void add_rec2(RunAcc& x, RunAcc& y, const float* r, float qx, float qy)
+    {
+        const float2 qqx = f2(qx, qx), qqy = f2(qy, qy);
+        const float4* w4 = reinterpret_cast<const float4*>(r);
+#pragma unroll
+        for (int k = 0; k < NP; k += 2) {
+            const float4 w = w4[k / 2];
+            x.a[k] = __ffma2_rn(f2(w.x, w.y), qqx, x.a[k]);
+            y.a[k] = __ffma2_rn(f2(w.x, w.y), qqy, y.a[k]);
+            if (k + 1 < NP) {
+                x.a[k + 1] = __ffma2_rn(f2(w.z, w.w), qqx, x.a[k + 1]);
+                y.a[k + 1] = __ffma2_rn(f2(w.z, w.w), qqy, y.a[k + 1]);
+            }
+        }
+    }
     __device__ __forceinline__ float get(int k) const { return (k & 1) ? a[k / 2].y : a[k / 2].x; }
 };
 
@@ -477,10 +493,7 @@ __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, 
         const float b = r[boff];
         const float qv0 = dir0 == 0 ? b : b * r[voff0];
         const float qv1 = b * r[voff1];
-        float w[SP];
-        load_weights<float, SP>(r, w);
-        acc0.add(w, qv0);
-        acc1.add(w, qv1);
+        RunAcc<float, S, SP>::add_rec2(acc0, acc1, r, qv0, qv1);
     }
     if (cur >= 0) flush(cur);
 }
