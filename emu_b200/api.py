@@ -168,8 +168,38 @@ class LocalGroup:
             self.h = None
 
 
+_nccl_preloaded = False
+
+
+def _preload_nccl():
+    """Load the NCCL of the nvidia-nccl wheel (the one PyTorch links) before
+    the library opens NCCL by its soname, so that one NCCL serves both: a
+    system libnccl.so.2 found first would satisfy PyTorch's later load of the
+    same soname and lack symbols PyTorch needs.  EMU_NCCL_LIBRARY names
+    another NCCL explicitly."""
+    global _nccl_preloaded
+    if _nccl_preloaded:
+        return
+    _nccl_preloaded = True
+    path = os.environ.get("EMU_NCCL_LIBRARY")
+    if not path:
+        import importlib.util
+        try:
+            spec = importlib.util.find_spec("nvidia.nccl")
+        except (ImportError, ValueError):
+            spec = None
+        for d in (spec.submodule_search_locations if spec and spec.submodule_search_locations else []):
+            cand = os.path.join(d, "lib", "libnccl.so.2")
+            if os.path.exists(cand):
+                path = cand
+                break
+    if path:
+        ctypes.CDLL(path, mode=ctypes.RTLD_GLOBAL)
+
+
 def comm_id():
     """a new communicator id (bytes) for Context.attach_comm"""
+    _preload_nccl()
     lib = load_library()
     buf = ctypes.create_string_buffer(COMM_ID_BYTES)
     _check(lib.emu_comm_id(buf), None, "emu_comm_id")
@@ -421,6 +451,7 @@ class Context:
     def attach_comm(self, comm_id, rank, nranks):
         """join a particle-sharding communicator (before load_particles)"""
         assert len(comm_id) == COMM_ID_BYTES
+        _preload_nccl()
         self._ck(self.lib.emu_attach_comm(self.h, comm_id, int(rank), int(nranks)), "emu_attach_comm")
 
     # ---- discrete adjoint (FP64 RK4) ----

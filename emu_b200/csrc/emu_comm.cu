@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -43,8 +44,11 @@ const NcclApi& nccl()
     static NcclApi api;
     static std::once_flag once;
     std::call_once(once, [] {
-        // an already loaded NCCL (e.g. the one PyTorch brought) is reused
-        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        // EMU_NCCL_LIBRARY names the NCCL to use; otherwise an already loaded
+        // NCCL (e.g. the one PyTorch brought) is reused by its soname
+        const char* path = getenv("EMU_NCCL_LIBRARY");
+        void* h = (path && *path) ? dlopen(path, RTLD_NOW | RTLD_GLOBAL) : nullptr;
+        if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
         if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
         if (!h) {
             api.why = std::string("cannot load libnccl.so.2: ") + dlerror();
