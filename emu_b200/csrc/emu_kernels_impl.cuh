@@ -1867,6 +1867,38 @@ __global__ void __launch_bounds__(kBlock) k_gather_deposit(DevParams P, DevState
                                             [](double a, int) -> double { return a; });
 }
 
+// The combined deposit (Comb<NF>) of a cell-sorted mixed state, one particle
+// per thread: the next step's first mesh after a re-sort.  Kept apart from
+// the gather (a lean kernel of many loads in flight) so that each runs at
+// its own occupancy.
+template <int NF, int WX, int WY, int WZ>
+__global__ void __launch_bounds__(kBlock) k_deposit_comb(DevParams P, DevState S, long long* __restrict__ qmesh)
+{
+    using SWt = SW<WX, WY, WZ>;
+    constexpr int NH = NF * NF, NS = 2 * NH;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = p < S.n;
+    Stencil<float> st{};
+    float fN[NS] = {};
+    float vx = 0, vy = 0, vz = 0;
+    if (active) {
+        make_stencil<float>(P, S.pos[0][p], S.pos[1][p], S.pos[2][p], st);
+        vx = S.vhat32[0][p];
+        vy = S.vhat32[1][p];
+        vz = S.vhat32[2][p];
+        const float N0 = S.N32[0][p], N1 = S.N32[1][p];
+#pragma unroll
+        for (int e = 0; e < NH; e++) {
+            fN[e] = (float)S.f0[e * S.cap + p] * N0;
+            fN[NH + e] = (float)S.f0[(NH + e) * S.cap + p] * N1;
+        }
+    }
+    float cN[Comb<NF>::NV];
+    combine_species<NF>(fN, cN);
+    tile_deposit_block<NF, SWt, float, long long, QuantConvG, true>(P, qmesh, active, st, cN, vx, vy, vz,
+                                                                    QuantConvG{P});
+}
+
 __global__ void k_mixed_shadow(DevState S)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2053,10 +2085,12 @@ void launch_gather_deposit_t(bool mixed, const DevParams& P, const DevState& src
 {
     EMU_W_DISPATCH(P, {
         if (mixed) {
+            // (mixed: the gather and the deposit as two kernels, each at its
+            // own occupancy)
+            k_gather_state<NF><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, 1);
             constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>();
-            smem_optin(k_gather_deposit<NF, WXv, WYv, WZv, true>, bytes);
-            k_gather_deposit<NF, WXv, WYv, WZv, true><<<grid_for(src.n), kBlock, bytes, st>>>(P, src, dst, perm,
-                                                                                             mesh, qmesh);
+            smem_optin(k_deposit_comb<NF, WXv, WYv, WZv>, bytes);
+            k_deposit_comb<NF, WXv, WYv, WZv><<<grid_for(src.n), kBlock, bytes, st>>>(P, dst, qmesh);
         } else {
             constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, double>();
             smem_optin(k_gather_deposit<NF, WXv, WYv, WZv, false>, bytes);
