@@ -79,6 +79,7 @@ void emu::make_devparams(const emu_params& p, DevParams& P)
     P.cfl_factor = p.cfl_factor;
     P.flavor_cfl_factor = p.flavor_cfl_factor;
     P.max_adaptive_speedup = p.max_adaptive_speedup;
+    P.m4_reduced = p.precision == EMU_PREC_MIXED && !(p.max_adaptive_speedup > 1.0);
     P.dt_translation = 0.0;
     if (p.cfl_factor > 0.0) P.dt_translation = std::min(std::min(dx[0], dx[1]), dx[2]) / emu::kC * p.cfl_factor;
     double m2[2][9];
@@ -227,6 +228,21 @@ int sync_ctl(emu_context* ctx)
     return EMU_OK;
 }
 
+// the mixed path's stage-4 mesh of the latest step in the full layout (a
+// step inside a longer run keeps only the combined layout there)
+int require_full_m4(emu_context* ctx, const char* what)
+{
+    if (!ctx->mixed || !ctx->P.m4_reduced || ctx->cur_mesh != 1) return EMU_OK;
+    int r;
+    if ((r = sync_ctl(ctx))) return r;
+    if (!ctx->ctl_host->m4_full)
+        return fail(ctx, EMU_ERR_STATE,
+                    std::string(what) + ": the latest step kept only the combined layout of its stage-4 mesh (a "
+                                        "step timed by emu_profile_step, or a run stopped by an error); take a step "
+                                        "with emu_evolve_steps or emu_step first");
+    return EMU_OK;
+}
+
 int status_of(emu_context* ctx, int64_t* bad)
 {
     const StepCtl& h = *ctx->ctl_host;
@@ -246,6 +262,8 @@ int status_of(emu_context* ctx, int64_t* bad)
 
 // ---- mesh helpers ----------------------------------------------------------
 long long mesh_elems(const emu_context* c) { return c->P.ncells * c->ND; }
+// an int64 mesh of the mixed path with its diagonal slots
+long long qmesh_elems(const emu_context* c) { return c->P.ncells * (c->ND + emu::kDiagSlots); }
 
 int zero_mesh(emu_context* ctx, int i)
 {
@@ -267,8 +285,23 @@ int deposit_full_q(emu_context* ctx)
 }
 
 // the full mesh of the mixed path that the API reads: the last deposit's
-// (after a load or emu_deposit) or the stage-4 mesh M_4 (after steps)
-long long* q_current(emu_context* ctx) { return ctx->cur_mesh == 0 ? ctx->qfull : ctx->qmesh[1]; }
+// (after a load or emu_deposit) or the stage-4 mesh M_4 (after steps: in
+// qfull with DevParams::m4_reduced, else in q[1])
+// stage 3's target for the full stage-4 mesh (DevParams::m4_reduced): qfull,
+// or this rank's part of it when sharded
+long long* m4_target(emu_context* ctx) { return ctx->qfull_part ? ctx->qfull_part : ctx->qfull; }
+
+// sharded: the ranks' parts of the latest full stage-4 mesh summed into qfull
+int sum_full_parts(emu_context* ctx)
+{
+    if (!ctx->qfull_part) return EMU_OK;
+    return emu_ctx::reduce_mesh_into(ctx, ctx->qfull_part, ctx->qfull, ctx->stream);
+}
+
+long long* q_current(emu_context* ctx)
+{
+    return (ctx->cur_mesh == 0 || ctx->P.m4_reduced) ? ctx->qfull : ctx->qmesh[1];
+}
 
 // deposit of the current state into mesh slot 0 and a clean slot 1: the
 // state the fused step loop expects at a step boundary (mixed path: the full
@@ -317,13 +350,16 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt, bool dep4
     int a = 0;
     for (int s = 1; s <= 4; s++) {
         const int b = 1 - a;
-        // M_1..M_3 in the combined layout, M_4 full
-        emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, s != 4, st);
-        // M_4 sits in q[1] (read by stage 4's compute_dt) until the next
-        // step's first finalize zeroes it
+        // M_1..M_3 in the combined layout; M_4 in q[1] (read by stage 4's
+        // compute_dt until the next step's first finalize zeroes it): full,
+        // or with DevParams::m4_reduced combined with the diagonal slots and
+        // the full layout in qfull on the steps after which it can be read
+        const bool comb = s != 4 || ctx->P.m4_reduced;
+        emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, comb,
+                                   (s == 3 && ctx->P.m4_reduced) ? m4_target(ctx) : nullptr, st);
         const bool dep = s < 4 || dep4;
         emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr, ctx->qmesh[1],
-                                    ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
+                                    m4_target(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
         int r;
         if (dep && (r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return r;
         a = b;
@@ -620,11 +656,11 @@ int emu_create(const emu_params* p, emu_context** out)
     e = cudaEventCreateWithFlags(&ctx->upload_done, cudaEventDisableTiming);
     if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return bail(EMU_ERR_CUDA); }
     ctx->stream = ctx->own;
-    const size_t me = (size_t)mesh_elems(ctx);
+    const size_t me = (size_t)mesh_elems(ctx), mq = (size_t)qmesh_elems(ctx);
     if (ctx->mixed) {
         for (int i = 0; i < 2 && !r; i++)
-            if (emu_ctx::dev_malloc(&ctx->qmesh[i], sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
-        if (!r && emu_ctx::dev_malloc(&ctx->qfull, sizeof(long long) * me) != cudaSuccess) r = EMU_ERR_NOMEM;
+            if (emu_ctx::dev_malloc(&ctx->qmesh[i], sizeof(long long) * mq) != cudaSuccess) r = EMU_ERR_NOMEM;
+        if (!r && emu_ctx::dev_malloc(&ctx->qfull, sizeof(long long) * mq) != cudaSuccess) r = EMU_ERR_NOMEM;
         if (!r && emu_ctx::dev_malloc(&ctx->gmesh, sizeof(float) * ctx->P.ncells * (ctx->nf == 3 ? emu::Comb<3>::NG : emu::Comb<2>::NG)) != cudaSuccess)
             r = EMU_ERR_NOMEM;
     } else {
@@ -646,8 +682,8 @@ int emu_create(const emu_params* p, emu_context** out)
     for (int i = 0; i < 4; i++)
         if (ctx->mesh[i] && e == cudaSuccess) e = cudaMemsetAsync(ctx->mesh[i], 0, sizeof(double) * me, ctx->own);
     for (int i = 0; i < 2; i++)
-        if (ctx->qmesh[i] && e == cudaSuccess) e = cudaMemsetAsync(ctx->qmesh[i], 0, sizeof(long long) * me, ctx->own);
-    if (ctx->qfull && e == cudaSuccess) e = cudaMemsetAsync(ctx->qfull, 0, sizeof(long long) * me, ctx->own);
+        if (ctx->qmesh[i] && e == cudaSuccess) e = cudaMemsetAsync(ctx->qmesh[i], 0, sizeof(long long) * mq, ctx->own);
+    if (ctx->qfull && e == cudaSuccess) e = cudaMemsetAsync(ctx->qfull, 0, sizeof(long long) * mq, ctx->own);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->own);
     if (e != cudaSuccess) {
         ctx->err = "emu_create: device initialisation failed";
@@ -668,6 +704,7 @@ void emu_destroy(emu_context* ctx)
     for (int i = 0; i < 4; i++) if (ctx->mesh[i]) emu_ctx::dev_free(ctx->mesh[i]);
     for (int i = 0; i < 2; i++) if (ctx->qmesh[i]) emu_ctx::dev_free(ctx->qmesh[i]);
     if (ctx->qfull) emu_ctx::dev_free(ctx->qfull);
+    if (ctx->qfull_part) emu_ctx::dev_free(ctx->qfull_part);
     if (ctx->gmesh) emu_ctx::dev_free(ctx->gmesh);
     if (ctx->fmesh_tmp) emu_ctx::dev_free(ctx->fmesh_tmp);
     if (ctx->planes) emu_ctx::dev_free(ctx->planes);
@@ -775,6 +812,7 @@ int emu_get_mesh(emu_context* ctx, double* out)
 {
     if (!ctx || !out) return fail(ctx, EMU_ERR_ARG, "emu_get_mesh: bad arguments");
     const long long nc = ctx->P.ncells;
+    if (int r0 = require_full_m4(ctx, "emu_get_mesh")) return r0;
     if (ctx->mixed) emu::launch_mesh_out_q(ctx->nf, ctx->P, q_current(ctx), ctx->planes, ctx->stream);
     else emu::launch_mesh_out(ctx->nf, ctx->P, ctx->mesh[ctx->cur_mesh], ctx->planes, ctx->stream);
     int r;
@@ -801,6 +839,7 @@ int emu_interpolate_rhs(emu_context* ctx, double* rhs_records)
         ctx->S[1].kgen = ctx->S[0].kgen;
     }
     const double* mesh = nullptr;
+    if (int r0 = require_full_m4(ctx, "emu_interpolate_rhs")) return r0;
     if (ctx->mixed) {
         // the FP64 interpolation of the fixed-point mesh
         if (!ctx->fmesh_tmp) CU(emu_ctx::dev_malloc(&ctx->fmesh_tmp, sizeof(double) * mesh_elems(ctx)));
@@ -837,7 +876,11 @@ int emu_compute_dt(emu_context* ctx, double* dt)
 {
     if (!ctx || !dt) return EMU_ERR_ARG;
     emu::launch_ctl_set(ctx->ctl, 0.0, 0.0, 0.0, 1, 1, ctx->stream);
-    if (ctx->mixed) emu::launch_dt_q(ctx->nf, ctx->P, q_current(ctx), ctx->ctl, emu::DT_QUERY, ctx->stream);
+    // (after steps: the diagonal slots the steps' compute_dt read)
+    if (ctx->mixed)
+        emu::launch_dt_q(ctx->nf, ctx->P, q_current(ctx),
+                         ctx->P.m4_reduced && ctx->cur_mesh == 1 ? ctx->qmesh[1] + mesh_elems(ctx) : nullptr, ctx->ctl,
+                         emu::DT_QUERY, ctx->stream);
     else emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[ctx->cur_mesh], ctx->ctl, emu::DT_QUERY, ctx->stream);
     int r;
     if ((r = check_launch(ctx, "compute_dt"))) return r;
@@ -865,6 +908,7 @@ int emu_step(emu_context* ctx, double dt, int64_t* bad)
             r = ctx->mixed ? enqueue_rk4_mixed(ctx, ctx->stream, false) : enqueue_rk4_fp64(ctx, ctx->stream, false);
         }
         if (r) return r;
+        if (ctx->mixed && (r = sum_full_parts(ctx))) return r;
         ctx->cur_mesh = ctx->mixed ? 1 : 3;
         ctx->fused_ready = true;
     } else {
@@ -888,8 +932,11 @@ int emu_evolve_begin(emu_context* ctx, double start_time, double end_time, int m
     if (ctx->mixed) {
         // the full mesh of the current state (after steps the step's first
         // mesh holds only the combined layout)
-        if (ctx->cur_mesh != 0 && (r = deposit_full_q(ctx))) return r;
-        emu::launch_dt_q(ctx->nf, ctx->P, ctx->qfull, ctx->ctl, emu::DT_INIT, ctx->stream);
+        if (ctx->cur_mesh != 0) {
+            if ((r = deposit_full_q(ctx))) return r;
+            ctx->cur_mesh = 0;   // qfull: the deposit of the current state
+        }
+        emu::launch_dt_q(ctx->nf, ctx->P, ctx->qfull, nullptr, ctx->ctl, emu::DT_INIT, ctx->stream);
     }
     else emu::launch_dt(ctx->nf, ctx->P, ctx->mesh[0], ctx->ctl, emu::DT_INIT, ctx->stream);
     return check_launch(ctx, "initial compute_dt");
@@ -899,6 +946,9 @@ int emu_evolve_steps(emu_context* ctx, int nsteps)
 {
     if (!ctx) return EMU_ERR_ARG;
     int r;
+    // the last of these steps deposits the full stage-4 mesh (the one a
+    // caller can read after the call)
+    if (ctx->mixed && ctx->P.m4_reduced && nsteps > 0) emu::launch_ctl_m4(ctx->ctl, nsteps, ctx->stream);
     for (int i = 0; i < nsteps; i++) {
         // when a re-sort follows this step, its gather makes the deposit of
         // the new state (in cell order) instead of the last stage
@@ -913,7 +963,7 @@ int emu_evolve_steps(emu_context* ctx, int nsteps)
             ctx->steps_since_sort++;
         }
     }
-    return EMU_OK;
+    return nsteps > 0 ? sum_full_parts(ctx) : EMU_OK;
 }
 
 int emu_evolve_end(emu_context* ctx, emu_run_info* info)
@@ -982,6 +1032,9 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
         return EMU_OK;
     }
     const int nk = ctx->mixed ? 8 : 4;
+    // timed as a step inside a longer run: the stage-4 mesh stays in the
+    // combined layout (DevParams::m4_reduced) unless the run ends here
+    if (ctx->mixed && ctx->P.m4_reduced) emu::launch_ctl_m4(ctx->ctl, 2, ctx->stream);
     const bool resort_due = ctx->prm.resort_interval > 0 && ctx->steps_since_sort + 1 >= ctx->prm.resort_interval;
     if (max_kernels < nk + (resort_due ? 1 : 0))
         return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
@@ -996,40 +1049,46 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
         for (int s = 1; s <= 4; s++) {
             const int b = 1 - a;
             rec(2 * k);
-            emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, s != 4,
-                                       st);
+            emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl,
+                                       s != 4 || ctx->P.m4_reduced,
+                                       (s == 3 && ctx->P.m4_reduced) ? m4_target(ctx) : nullptr, st);
             rec(2 * k + 1);
             k++;
+            // as in the evolve loop: a re-sort that follows makes the
+            // deposit of the new state instead of stage 4
+            const bool dep = s < 4 || !resort_due;
             rec(2 * k);
-            emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, ctx->qmesh[b], ctx->qmesh[1], ctx->ctl,
-                                        s == 4 ? emu::DT_ADVANCE : -1, st);
+            emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr,
+                                        ctx->qmesh[1], m4_target(ctx), ctx->ctl, s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
             int rr;
-            if ((rr = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return rr;
+            if (dep && (rr = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return rr;
             a = b;
         }
     } else {
         for (int s = 1; s <= 4; s++) {
+            const bool dep = s < 4 || !resort_due;
             rec(2 * k);
-            emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], ctx->mesh[s % 4],
+            emu::launch_rk4_stage(ctx->nf, ctx->P, S, s, ctx->mesh[s - 1], dep ? ctx->mesh[s % 4] : nullptr,
                                   ctx->mesh[(s + 1) % 4], mesh_elems(ctx), ctx->ctl,
                                   s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
             int rr;
-            if ((rr = emu_ctx::reduce_mesh(ctx, ctx->mesh[s % 4], false, st))) return rr;
+            if (dep && (rr = emu_ctx::reduce_mesh(ctx, ctx->mesh[s % 4], false, st))) return rr;
         }
     }
     int r = check_launch(ctx, "profile step");
     if (r) return r;
+    if (ctx->mixed && (r = sum_full_parts(ctx))) return r;
     ctx->cur_mesh = ctx->mixed ? 1 : 3;
     if (ctx->prm.resort_interval > 0) ctx->steps_since_sort++;
     if (resort_due) {
-        // the re-sort that follows the step (keys, radix sort, gather) as
-        // one more entry
+        // the re-sort that follows the step (keys, radix sort, gather and
+        // the deposit of the new state) as one more entry
         rec(2 * k);
-        if ((r = resort(ctx))) return r;
+        if ((r = resort(ctx, true))) return r;
         rec(2 * k + 1);
         k++;
     }

@@ -138,13 +138,13 @@ __global__ void k_sum_ranks(T* __restrict__ out, RankPtrs in, int nranks, long l
     }
 }
 
-int local_reduce_mesh(emu_context* ctx, void* mesh, bool int64, size_t count, cudaStream_t st)
+int local_reduce_mesh(emu_context* ctx, const void* src, void* mesh, bool int64, size_t count, cudaStream_t st)
 {
     LocalGroup& g = *static_cast<LocalGroup*>(ctx->local);
     const int r = ctx->rank;
     if (count * 8 > g.bytes) return fail(ctx, EMU_ERR_STATE, "local group: mesh larger than the send buffers");
     for (int k = 0; k < g.nranks; k++) CU(cudaStreamWaitEvent(st, g.done[k], 0));
-    CU(cudaMemcpyAsync(g.send[r], mesh, count * 8, cudaMemcpyDeviceToDevice, st));
+    CU(cudaMemcpyAsync(g.send[r], src, count * 8, cudaMemcpyDeviceToDevice, st));
     CU(cudaEventRecord(g.ready[r], st));
     if (!rendezvous(g)) return fail(ctx, EMU_ERR_STATE, "local group: a rank did not reach the mesh reduction");
     RankPtrs ptrs{};
@@ -185,12 +185,33 @@ int local_reduce_scalars(emu_context* ctx, double* v, int n, int op)
 
 int emu_ctx::reduce_mesh(emu_context* ctx, void* mesh, bool int64, cudaStream_t st)
 {
-    if (ctx->local) return local_reduce_mesh(ctx, mesh, int64, (size_t)ctx->P.ncells * ctx->ND, st);
+    // (the mixed path's int64 meshes with their diagonal slots)
+    const size_t count = (size_t)ctx->P.ncells * (ctx->ND + (int64 ? emu::kDiagSlots : 0));
+    if (ctx->local) return local_reduce_mesh(ctx, mesh, mesh, int64, count, st);
     if (!ctx->comm) return EMU_OK;
-    const size_t count = (size_t)ctx->P.ncells * ctx->ND;
     ncclResult_t r = nccl().AllReduce(mesh, mesh, count, int64 ? ncclInt64 : ncclFloat64, ncclSum,
                                       static_cast<ncclComm_t>(ctx->comm), st);
     return r == ncclSuccess ? EMU_OK : nccl_fail(ctx, r, "mesh all-reduce");
+}
+
+// a sharded mixed context's part of the full stage-4 mesh
+static int alloc_full_part(emu_context* ctx)
+{
+    if (!ctx->mixed || !ctx->P.m4_reduced || ctx->qfull_part) return EMU_OK;
+    const size_t bytes = sizeof(long long) * (size_t)ctx->P.ncells * ctx->ND;
+    if (emu_ctx::dev_malloc(&ctx->qfull_part, bytes) != cudaSuccess)
+        return fail(ctx, EMU_ERR_NOMEM, "attach: full mesh part");
+    CU(cudaMemsetAsync(ctx->qfull_part, 0, bytes, ctx->stream));
+    return EMU_OK;
+}
+
+int emu_ctx::reduce_mesh_into(emu_context* ctx, const long long* src, long long* dst, cudaStream_t st)
+{
+    const size_t count = (size_t)ctx->P.ncells * ctx->ND;
+    if (ctx->local) return local_reduce_mesh(ctx, src, dst, true, count, st);
+    if (!ctx->comm) return EMU_OK;
+    ncclResult_t r = nccl().AllReduce(src, dst, count, ncclInt64, ncclSum, static_cast<ncclComm_t>(ctx->comm), st);
+    return r == ncclSuccess ? EMU_OK : nccl_fail(ctx, r, "full mesh all-reduce");
 }
 
 // sum (op 0) or max (op 1) of host scalars over the ranks; synchronous
@@ -249,6 +270,7 @@ int emu_attach_comm(emu_context* ctx, const char* id, int rank, int nranks)
     ctx->comm = c;
     ctx->rank = rank;
     ctx->nranks = nranks;
+    if (int e = alloc_full_part(ctx)) return e;
     CU(emu_ctx::dev_malloc(&ctx->red_scratch, 8 * sizeof(double)));
     return EMU_OK;
 }
@@ -292,7 +314,7 @@ int emu_attach_local(emu_context* ctx, void* group, int rank)
     if (!ctx || !g || rank < 0 || rank >= g->nranks) return fail(ctx, EMU_ERR_ARG, "emu_attach_local: bad arguments");
     if (ctx->comm || ctx->local) return fail(ctx, EMU_ERR_STATE, "emu_attach_local: a communicator is already attached");
     if (ctx->loaded) return fail(ctx, EMU_ERR_STATE, "emu_attach_local: attach before loading particles");
-    const size_t bytes = (size_t)ctx->P.ncells * ctx->ND * 8;
+    const size_t bytes = (size_t)ctx->P.ncells * (ctx->ND + emu::kDiagSlots) * 8;
     {
         std::lock_guard<std::mutex> lk(g->mu);
         if (g->send[rank]) return fail(ctx, EMU_ERR_STATE, "emu_attach_local: rank already attached");
@@ -305,6 +327,7 @@ int emu_attach_local(emu_context* ctx, void* group, int rank)
     ctx->local = g;
     ctx->rank = rank;
     ctx->nranks = g->nranks;
+    if (int e = alloc_full_part(ctx)) return e;
     return EMU_OK;
 }
 

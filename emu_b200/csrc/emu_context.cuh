@@ -35,6 +35,11 @@ struct emu_context {
     // (the step meshes M_1..M_3 hold only the combined self-interaction
     // layout; M_4 and this one are full, for compute_dt and the outputs)
     long long* qfull = nullptr;
+    // sharded mixed path with DevParams::m4_reduced: this rank's part of the
+    // full stage-4 mesh, summed into qfull after each emu_evolve_steps (the
+    // device decides which steps deposit it; the sum of the latest parts is
+    // the same however often it is taken)
+    long long* qfull_part = nullptr;
     float* gmesh = nullptr;
     double* fmesh_tmp = nullptr;        // FP64 cell-major copy (mixed API calls)
     double* planes = nullptr;           // ncomp x ncells output staging
@@ -111,6 +116,8 @@ int step_device(emu_context* ctx, bool last_stage_deposit = true);
 // sum a deposited mesh (FP64, or int64 for the mixed path) over the ranks of
 // the attached communicator, enqueued on st; no-op without one
 int reduce_mesh(emu_context* ctx, void* mesh, bool int64, cudaStream_t st);
+// sum the ranks' full int64 meshes src into dst (ncells * 8 NF^2 values)
+int reduce_mesh_into(emu_context* ctx, const long long* src, long long* dst, cudaStream_t st);
 }  // namespace emu_ctx
 // sum (op 0) or max (op 1) of n <= 8 host scalars over the ranks (synchronous)
 int emu_ctx_reduce_scalars(emu_context* ctx, double* v, int n, int op);

@@ -81,7 +81,17 @@ struct DevParams {
     double q_scale[2];        // contribution * q_scale -> integer
     double q_unscale[2];      // integer * q_unscale -> number (same units as FP64 mesh)
     long long wait_polls;     // polls of a grid-barrier wait before it gives up (ST_TIMEOUT)
+    // mixed path, compute_dt without the adaptive branch (max_adaptive_speedup
+    // <= 1, Evolve.cpp:64-71): the only stage-4 mesh values compute_dt reads
+    // are the diagonal N_ii, Nbar_ii (V_stupid, generate_code.py:287-293).  They are deposited apart (kDiagSlots per
+    // cell after the mesh), and the stage-4 mesh is deposited in full only
+    // where it can be read (see StepCtl::m4_full_from)
+    int m4_reduced;
 };
+
+// the diagonal number densities of a cell apart from its mesh: N_ii
+// (i < NF) then Nbar_ii, padded to eight int64 slots
+constexpr int kDiagSlots = 8;
 
 // ---------------------------------------------------------------------------
 // ParticleInterpolator (Source/ParticleInterpolator.H:34-131).  The nearest
@@ -583,6 +593,64 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
         }
         if (key < 0) continue;
         add_one(i);
+    }
+    if (cur >= 0) flush(cur);
+}
+
+// Deposit of the diagonal number densities N_ii, Nbar_ii (weight 1) into
+// diag[cell * kDiagSlots + c], c = sp * NF + i, from the CTA's FP32 records
+// (written for a full or a combined deposit, which has just read them; no
+// barrier is needed, the records are only read).  The record holds the
+// value of slot c at SP + voff(c): the particle's f N in the full layout,
+// the values after the NV combinations in the combined one.  Eight threads
+// per record stream (BLOCK / 8 streams of NTILE / (BLOCK / 8) records): the
+// grouping of the FP32 run sums, and so the int64 results, do not depend on
+// which layout the records have.
+template <int NF, int BLOCK, int NTILE, class SWt, class T, class Conv>
+__device__ __forceinline__ void tile_deposit_diag(const DevParams& P, T* diag, const int* skey, const float* srec,
+                                                  int ntile, bool comb_layout, Conv conv)
+{
+    using TR = TileRec<NF, SWt, float>;
+    using H = Herm<NF>;
+    constexpr int NH = NF * NF, RW = TR::RW, SP = TR::SP, S = TR::S;
+    constexpr int NSTREAM = BLOCK / kDiagSlots;
+    constexpr int CH = (NTILE + NSTREAM - 1) / NSTREAM;
+    static_assert(2 * NF <= kDiagSlots, "diagonal slots");
+    const int c = threadIdx.x % kDiagSlots;
+    const int stream = threadIdx.x / kDiagSlots;
+    if (stream >= NSTREAM || c >= 2 * NF) return;   // no block-wide barrier follows inside
+    const int sp = c / NF, i = c % NF;
+    const int voff = SP + (comb_layout ? Comb<NF>::NV + c : sp * NH + H::re(i, i));
+    RunAcc<float, S, SP> acc;
+    auto flush = [&](int key) {
+        const int bx = key % P.n[0];
+        const int by = (key / P.n[0]) % P.n[1];
+        const int bz = key / (P.n[0] * P.n[1]);
+#pragma unroll
+        for (int kk = 0; kk < SWt::MZ; kk++)
+#pragma unroll
+            for (int jj = 0; jj < SWt::MY; jj++)
+#pragma unroll
+                for (int ii = 0; ii < SWt::MX; ii++) {
+                    if (!SWt::on(P, ii, jj, kk)) continue;
+                    const int k = (kk * SWt::MY + jj) * SWt::MX + ii;
+                    const T v = conv(acc.get(k), sp);
+                    if (v != (T)0) atomic_add_mesh(&diag[cell_of(P, bx, by, bz, ii, jj, kk) * kDiagSlots + c], v);
+                }
+    };
+    const int i1 = min((stream + 1) * CH, ntile);
+    int cur = -1;
+    acc.zero();
+    for (int r = stream * CH; r < i1; r++) {
+        const int key = skey[r];
+        if (key != cur) {
+            if (cur >= 0) flush(cur);
+            acc.zero();
+            cur = key;
+        }
+        if (key < 0) continue;
+        const float* rec = srec + r * RW;
+        acc.add_rec(rec, rec[voff]);
     }
     if (cur >= 0) flush(cur);
 }

@@ -14,7 +14,8 @@ namespace emu {
     extern template void launch_rhs_t<NF>(const DevParams&, const DevState&, const double*, const double*,       \
                                           double*, cudaStream_t);                                                \
     extern template void launch_rk4_stage_mixed_t<NF>(const DevParams&, const DevState&, int, const float*,      \
-                                                      long long*, const long long*, StepCtl*, int, cudaStream_t); \
+                                                      long long*, const long long*, long long*, StepCtl*, int,   \
+                                                      cudaStream_t);                                             \
     extern template void launch_deposit_q_t<NF>(const DevParams&, const DevState&, const double*, long long*,    \
                                                 cudaStream_t);                                                   \
     extern template bool coop_step_fits_t<NF>(const DevParams&, long long);                                      \
@@ -129,11 +130,11 @@ cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, 
 }
 
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
-                            long long* qmesh_out, const long long* qmesh_dt, StepCtl* ctl, int dt_mode,
-                            cudaStream_t st)
+                            long long* qmesh_out, const long long* qmesh_dt, long long* qmesh_m4, StepCtl* ctl,
+                            int dt_mode, cudaStream_t st)
 {
-    if (nf == 2) launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, ctl, dt_mode, st);
-    else launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, ctl, dt_mode, st);
+    if (nf == 2) launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st);
+    else launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st);
 }
 
 static unsigned reduce_grid(long long ncells)
@@ -145,15 +146,15 @@ static unsigned reduce_grid(long long ncells)
 }
 
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
-                           StepCtl* ctl, bool comb, cudaStream_t st)
+                           StepCtl* ctl, bool comb, long long* qzero_m4, cudaStream_t st)
 {
     EMU_NF_DISPATCH(nf, (launch_pdl(k_finalize_mixed<NFv>, reduce_grid(P.ncells * Comb<NFv>::NG), kBlock, 0, st, P,
-                                    qread, qzero, gmesh, ctl, comb ? 1 : 0)));
+                                    qread, qzero, gmesh, ctl, comb ? 1 : 0, qzero_m4)));
 }
 
 void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st)
 {
-    EMU_NF_DISPATCH(nf, (k_dt<NFv, double><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode)));
+    EMU_NF_DISPATCH(nf, (k_dt<NFv, double><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode, nullptr)));
 }
 
 void launch_full_to_comb(int nf, const DevParams& P, const long long* qfull, long long* qcomb, cudaStream_t st)
@@ -162,9 +163,10 @@ void launch_full_to_comb(int nf, const DevParams& P, const long long* qfull, lon
                                                                                                         qcomb)));
 }
 
-void launch_dt_q(int nf, const DevParams& P, const long long* mesh, StepCtl* ctl, int mode, cudaStream_t st)
+void launch_dt_q(int nf, const DevParams& P, const long long* mesh, const long long* diag, StepCtl* ctl, int mode,
+                 cudaStream_t st)
 {
-    EMU_NF_DISPATCH(nf, (k_dt<NFv, long long><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode)));
+    EMU_NF_DISPATCH(nf, (k_dt<NFv, long long><<<reduce_grid(P.ncells), kBlock, 0, st>>>(P, mesh, ctl, mode, diag)));
 }
 
 void launch_renorm(int nf, const DevParams& P, const DevState& S, StepCtl* ctl, cudaStream_t st)
@@ -193,6 +195,11 @@ void launch_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_
                     cudaStream_t st)
 {
     k_ctl_set<<<1, 1, 0, st>>>(ctl, dt, t, end_time, max_step, reset_status);
+}
+
+void launch_ctl_m4(StepCtl* ctl, int nsteps, cudaStream_t st)
+{
+    k_ctl_m4<<<1, 1, 0, st>>>(ctl, nsteps);
 }
 
 void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st)

@@ -12,7 +12,9 @@
 //   vhat32[3], N32[2]  mixed copies of the static fields           FP32
 //   id           load index of each particle                       int64
 // Meshes are cell-major: mesh[cell*ND + q] with q in GIdx order minus 3
-// (ND = 8*NF*NF), FP64 (plain) or int64 fixed point (mixed).
+// (ND = 8*NF*NF), FP64 (plain) or int64 fixed point (mixed).  The mixed
+// path's int64 meshes are followed by kDiagSlots per cell (the diagonal
+// N_ii, Nbar_ii that compute_dt reads, at mesh + ncells*ND).
 #pragma once
 
 #include "emu_device.cuh"
@@ -65,6 +67,14 @@ struct StepCtl {
     unsigned long long vmax_bits[2];   // max V_adaptive, V_stupid (non-negative doubles as bits)
     unsigned int bar_count, bar_gen;   // grid barrier of the cooperative step kernel
     double* dt_hist;     // when set: dt of step k is written to dt_hist[k] (recorded runs)
+    // mixed path with DevParams::m4_reduced: stage 3 deposits the stage-4
+    // mesh in full (the layout get_mesh and plotfiles read) from step
+    // m4_full_from on and on the final step of a run, and otherwise only the
+    // combined layout stage 4 interpolates; the diagonal N_ii compute_dt
+    // reads are deposited apart in both cases.  m4_full: whether the latest
+    // stage-3 deposit was the full one.
+    int m4_full_from;
+    int m4_full;
 };
 
 enum DtMode : int { DT_QUERY = 0, DT_INIT = 1, DT_ADVANCE = 2 };
@@ -99,16 +109,23 @@ void launch_rk4_stage(int nf, const DevParams& P, const DevState& S, int s, cons
 bool coop_step_fits(int nf, const DevParams& P, long long n);
 cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, double* const mesh[4], long long nmesh,
                                  StepCtl* ctl, int dt_mode, cudaStream_t st);
+// qmesh_m4: stage 3's target for the full stage-4 mesh (DevParams::m4_reduced)
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
-                            long long* qmesh_out, const long long* qmesh_dt, StepCtl* ctl, int dt_mode,
-                            cudaStream_t st);
-// comb: qread holds the combined layout (else the full mesh)
+                            long long* qmesh_out, const long long* qmesh_dt, long long* qmesh_m4, StepCtl* ctl,
+                            int dt_mode, cudaStream_t st);
+// comb: qread holds the combined layout (else the full mesh).  qzero is
+// zeroed with its diagonal slots (ncells * (8 NF^2 + kDiagSlots)); qzero_m4
+// (before stage 3, or nullptr) on the steps that deposit the full stage-4
+// mesh there (StepCtl::m4_full_from).
 void launch_finalize_mixed(int nf, const DevParams& P, const long long* qread, long long* qzero, float* gmesh,
-                           StepCtl* ctl, bool comb, cudaStream_t st);
+                           StepCtl* ctl, bool comb, long long* qzero_m4, cudaStream_t st);
 void launch_dt(int nf, const DevParams& P, const double* mesh, StepCtl* ctl, int mode, cudaStream_t st);
 // a full int64 mesh in the combined layout (mixed path)
 void launch_full_to_comb(int nf, const DevParams& P, const long long* qfull, long long* qcomb, cudaStream_t st);
-void launch_dt_q(int nf, const DevParams& P, const long long* mesh, StepCtl* ctl, int mode, cudaStream_t st);
+// diag: the mesh's diagonal slots (DevParams::m4_reduced), or nullptr to
+// read the full mesh
+void launch_dt_q(int nf, const DevParams& P, const long long* mesh, const long long* diag, StepCtl* ctl, int mode,
+                 cudaStream_t st);
 void launch_renorm(int nf, const DevParams& P, const DevState& S, StepCtl* ctl, cudaStream_t st);
 void launch_mesh_out(int nf, const DevParams& P, const double* mesh, double* out, cudaStream_t st);
 void launch_mesh_out_q(int nf, const DevParams& P, const long long* mesh, double* out, cudaStream_t st);
@@ -116,6 +133,8 @@ void launch_q_to_f64(int nf, const DevParams& P, const long long* mesh, double* 
 void launch_ctl_hist(StepCtl* ctl, double* hist, cudaStream_t st);
 void launch_ctl_set(StepCtl* ctl, double dt, double t, double end_time, int max_step, int reset_status,
                     cudaStream_t st);
+// the next nsteps steps: the last of them deposits the full stage-4 mesh
+void launch_ctl_m4(StepCtl* ctl, int nsteps, cudaStream_t st);
 void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st);
 void launch_flush(double* buf, long long n, cudaStream_t st);
 // cell re-sort: keys of the current positions, then gather every array

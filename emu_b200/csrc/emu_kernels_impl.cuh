@@ -270,6 +270,27 @@ __device__ __forceinline__ void cell_potentials(const DevParams& P, Get get, dou
     Vs = vs * (2.0 * NF * M_SQRT2 * P.GF / P.cell_volume);
 }
 
+// the step in progress deposits the full stage-4 mesh (DevParams::m4_reduced)
+__device__ __forceinline__ bool m4_full_step(const StepCtl* ctl)
+{
+    return ctl->step >= ctl->m4_full_from || ctl->last || ctl->step + 1 >= ctl->max_step;
+}
+
+// V_stupid of a cell from its diagonal slots (the operations of
+// cell_potentials on the same values)
+template <int NF>
+__device__ __forceinline__ void cell_vstupid(const DevParams& P, const long long* d, double& Vs)
+{
+    double vs = 0.0;
+#pragma unroll
+    for (int i = 0; i < NF; i++) {
+        vs = fmax(vs, (double)d[i] * P.q_unscale[0]);
+        vs = fmax(vs, (double)d[NF + i] * P.q_unscale[1]);
+    }
+    vs = fmax(vs, P.cell_volume * P.Ye * P.rho / kMp);
+    Vs = vs * (2.0 * NF * M_SQRT2 * P.GF / P.cell_volume);
+}
+
 // the last block to finish turns the reduced potentials into the next dt
 __device__ void dt_finish(const DevParams& P, StepCtl* ctl, int mode)
 {
@@ -324,7 +345,8 @@ __device__ __forceinline__ double mesh_value<long long>(const DevParams& P, cons
 // part in the cell reduction.
 template <int NF, class T>
 __device__ __forceinline__ void dt_reduce_and_finish(const DevParams& P, const T* __restrict__ mesh, StepCtl* ctl,
-                                                     int mode, unsigned ncb)
+                                                     int mode, unsigned ncb,
+                                                     const long long* __restrict__ diag = nullptr)
 {
     constexpr int NH = NF * NF, ND = 8 * NH;
     double va = 0.0, vs = 0.0;
@@ -332,9 +354,14 @@ __device__ __forceinline__ void dt_reduce_and_finish(const DevParams& P, const T
         // cell c goes to block c % ncb: every block takes a few cells
         const long long stride = (long long)ncb * blockDim.x;
         for (long long c = blockIdx.x + (long long)ncb * threadIdx.x; c < P.ncells; c += stride) {
-            const T* m = mesh + c * ND;
-            double a, b;
-            cell_potentials<NF>(P, [&](int q) { return mesh_value<T>(P, m, q, NH); }, a, b);
+            double a = 0.0, b;
+            if (diag) {
+                // V_stupid from the diagonal slots (V_adaptive is not used)
+                cell_vstupid<NF>(P, diag + c * kDiagSlots, b);
+            } else {
+                const T* m = mesh + c * ND;
+                cell_potentials<NF>(P, [&](int q) { return mesh_value<T>(P, m, q, NH); }, a, b);
+            }
             va = fmax(va, a);
             vs = fmax(vs, b);
         }
@@ -505,11 +532,12 @@ __device__ __forceinline__ bool distinct_key_rank(int key, int* scratch, int& sl
 // that moved since the last re-sort; the deposit of moved particles at the
 // end of a step): the 128 keys are ranked first (stable, so cell-sorted
 // particles keep their order), so that each stencil forms one run
-// COMB: the mixed path's combined deposit (fN holds the NF^2 combinations)
+// COMB: the mixed path's combined deposit (fN holds the Comb<NF> values;
+// NREC > NV: further values the records carry for a later pass)
 // given_slot >= 0 (in every thread, or in none): the record slots are given
 // (a rank made earlier for the same keys) and no ranking is done.  Returns
 // the thread's slot.
-template <int NF, class SWt, class R, class T, class Conv, bool COMB = false>
+template <int NF, class SWt, class R, class T, class Conv, bool COMB = false, int NREC = Comb<NF>::NV>
 __device__ __forceinline__ int tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
                                                   const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false,
                                                   int given_slot = -1)
@@ -543,7 +571,7 @@ __device__ __forceinline__ int tile_deposit_block(const DevParams& P, T* mesh, b
         }
     }
     if constexpr (COMB) {
-        tile_record<NF, SWt, R, Comb<NF>::NV>(srec, skey, slot, key, fN, vx, vy, vz, st);
+        tile_record<NF, SWt, R, NREC>(srec, skey, slot, key, fN, vx, vy, vz, st);
         __syncthreads();
         tile_deposit_comb<NF, kBlock, kBlock, SWt, T>(P, mesh, skey, srec, kBlock, conv);
     } else {
@@ -1136,10 +1164,11 @@ __global__ void __launch_bounds__(kBlock) k_renorm(DevParams P, DevState S, Step
 
 // compute_dt for host-driven calls and the initial dt of a run
 template <int NF, class T>
-__global__ void __launch_bounds__(kBlock) k_dt(DevParams P, const T* __restrict__ mesh, StepCtl* ctl, int mode)
+__global__ void __launch_bounds__(kBlock) k_dt(DevParams P, const T* __restrict__ mesh, StepCtl* ctl, int mode,
+                                               const long long* __restrict__ diag)
 {
     if (mode == DT_ADVANCE && ctl->done) return;
-    dt_reduce_and_finish<NF, T>(P, mesh, ctl, mode, gridDim.x);
+    dt_reduce_and_finish<NF, T>(P, mesh, ctl, mode, gridDim.x, diag);
 }
 
 // ===========================================================================
@@ -1152,7 +1181,7 @@ __global__ void __launch_bounds__(kBlock) k_dt(DevParams P, const T* __restrict_
 template <int NF>
 __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const long long* __restrict__ q,
                                                            long long* __restrict__ qzero, float* __restrict__ g,
-                                                           StepCtl* ctl, int comb)
+                                                           StepCtl* ctl, int comb, long long* __restrict__ qzero_m4)
 {
     using H = Herm<NF>;
     using C = Comb<NF>;
@@ -1160,7 +1189,10 @@ __global__ void __launch_bounds__(kBlock) k_finalize_mixed(DevParams P, const lo
     grid_dep_wait();   // the previous stage's deposit is complete
     grid_dep_launch();
     if (ctl->done) return;
-    zero_slice(qzero, qzero ? P.ncells * ND : 0);
+    zero_slice(qzero, qzero ? P.ncells * (ND + kDiagSlots) : 0);
+    // (before stage 3: the full stage-4 mesh's target, on the steps that
+    // deposit it)
+    if (qzero_m4 && m4_full_step(ctl)) zero_slice(qzero_m4, P.ncells * ND);
     const long long stride = (long long)gridDim.x * blockDim.x;
     if (comb) {
         // a combined mesh holds the values of G itself
@@ -1365,7 +1397,8 @@ template <int NF, int WX, int WY, int WZ>
 __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S, int s,
                                                             const float* __restrict__ gmesh,
                                                             long long* __restrict__ qout,
-                                                            const long long* __restrict__ qdt, StepCtl* ctl,
+                                                            const long long* __restrict__ qdt,
+                                                            long long* __restrict__ qm4, StepCtl* ctl,
                                                             int dt_mode)
 {
     using H = Herm<NF>;
@@ -1511,10 +1544,11 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         }
     }
     // compute_dt on the stage-4 mesh (every block has read this step's dt)
-    if (dt_mode == DT_ADVANCE) dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P));
+    if (dt_mode == DT_ADVANCE)
+        dt_reduce_and_finish<NF, long long>(P, qdt, ctl, DT_ADVANCE, reduce_blocks(P),
+                                            P.m4_reduced ? qdt + P.ncells * (8 * NH) : nullptr);
     if (active) {
         // the state arrays never alias
-        const double* __restrict__ f0p = S.f0;
         const float* __restrict__ k32p = S.k32;
         const float* __restrict__ ks32p = S.ksum32;
         if constexpr (PRELOAD) {
@@ -1670,10 +1704,34 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     if (qout) {
         // (stages 1-3: the rank the last stage 4 stored, see rk4_stage_body)
         const int given = (s < 4 && P.rank_stages) ? (active ? S.rslot[p] : t) : -1;
-        if (s == 3) {
-            // M_4, the mesh compute_dt reads (N, Nbar and the fluxes apart):
-            // the full layout
+        if (s == 3 && !P.m4_reduced) {
+            // M_4 in the full layout (N, Nbar and the fluxes apart): compute_dt
+            // reads more of it than the diagonal
             tile_deposit_block<NF, SWt, float>(P, qout, live, st, fN, vx, vy, vz, QuantConv{P}, false, given);
+        } else if (s == 3) {
+            // M_4: the combined layout stage 4 interpolates, the diagonal N_ii
+            // compute_dt reads apart, and the full layout (into qm4) only on
+            // the steps after which it can be read
+            constexpr int NV = Comb<NF>::NV;
+            float cN[NV + 2 * NF];
+            combine_species<NF>(fN, cN);
+#pragma unroll
+            for (int i = 0; i < NF; i++) {
+                cN[NV + i] = fN[H::re(i, i)];
+                cN[NV + NF + i] = fN[NH + H::re(i, i)];
+            }
+            const int sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true, NV + 2 * NF>(
+                P, qout, live, st, cN, vx, vy, vz, QuantConvG{P}, false, given);
+            // (the records the deposit above has read, still in place)
+            tile_deposit_diag<NF, kBlock, kBlock, SWt, long long>(
+                P, qout + P.ncells * (8 * NH), reinterpret_cast<const int*>(tile_smem),
+                reinterpret_cast<const float*>(tile_smem + kBlock * 8), kBlock, true, QuantConv{P});
+            const bool full = m4_full_step(ctl);   // uniform over the grid
+            if (full) {
+                __syncthreads();   // every record has been read
+                tile_deposit_block<NF, SWt, float>(P, qm4, live, st, fN, vx, vy, vz, QuantConv{P}, false, sl);
+            }
+            if (blockIdx.x == 0 && t == 0) ctl->m4_full = full ? 1 : 0;
         } else {
             // M_2, M_3 and the next step's M_1: only the combinations the
             // stages interpolate
@@ -1954,10 +2012,16 @@ __global__ void k_ctl_set(StepCtl* ctl, double dt, double t, double end_time, in
     ctl->bar_count = 0u;
     ctl->bar_gen = 0u;
     ctl->dt_hist = nullptr;
+    ctl->m4_full_from = 0;
     if (reset_status) {
         ctl->status = 0;
         ctl->bad = LLONG_MAX;
     }
+}
+
+__global__ void k_ctl_m4(StepCtl* ctl, int nsteps)
+{
+    ctl->m4_full_from = ctl->step + nsteps - 1;
 }
 
 __global__ void k_flush(double* buf, long long n)
@@ -2119,13 +2183,13 @@ void launch_rhs_t(const DevParams& P, const DevState& S, const double* f, const 
 
 template <int NF>
 void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, const float* gmesh, long long* qout,
-                              const long long* qdt, StepCtl* ctl, int dt_mode, cudaStream_t st)
+                              const long long* qdt, long long* qm4, StepCtl* ctl, int dt_mode, cudaStream_t st)
 {
     EMU_W_DISPATCH(P, {
         constexpr int bytes = mixed_stage_smem_bytes<NF, WXv, WYv, WZv>();
         smem_optin(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, bytes);
         launch_pdl(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock, bytes, st, P, S, s, gmesh, qout, qdt,
-                   ctl, dt_mode);
+                   qm4, ctl, dt_mode);
     });
 }
 

@@ -171,7 +171,10 @@ int emu_num_particles(const emu_context* ctx, int64_t* n);
 
 /* deposit_to_mesh (Evolve.H:31 / Evolve.cpp:91-126) of the current particles */
 int emu_deposit(emu_context* ctx);
-/* The current mesh (rho,T,Ye and the last deposit), GIdx planes. */
+/* The current mesh (rho,T,Ye and the last deposit), GIdx planes.  After
+ * steps: the deposit of the last step's stage-4 state, as the reference's
+ * state MultiFab holds it.  (Mixed precision: EMU_ERR_STATE after a step
+ * timed by emu_profile_step, which keeps only the layout stage 4 reads.) */
 int emu_get_mesh(emu_context* ctx, double* out);
 /* interpolate_rhs_from_mesh (Evolve.H:33 / Evolve.cpp:128-176): the time
  * derivative of every attribute of every particle, from the current mesh,
@@ -197,6 +200,12 @@ int emu_evolve(emu_context* ctx, int nsteps, double start_time, double end_time,
  * many steps (each a CUDA graph launch, no host synchronisation); end =
  * synchronise and report.  Steps past max_steps or end_time do no work. */
 int emu_evolve_begin(emu_context* ctx, double start_time, double end_time, int max_steps);
+/* Mixed precision without the adaptive timestep branch (max_adaptive_speedup
+ * <= 1): the steps of one call but the last (and the last of the run) keep
+ * their stage-4 mesh only in the layout stage 4 interpolates, plus the
+ * diagonal N_ii that compute_dt reads, none of which a caller can read
+ * before the call returns; the results do not depend on how a run is split
+ * into calls. */
 int emu_evolve_steps(emu_context* ctx, int nsteps);
 int emu_evolve_end(emu_context* ctx, emu_run_info* info);
 /* Limit of the bounded grid-barrier waits of this context's cooperative
@@ -211,13 +220,15 @@ int emu_set_wait_limit(emu_context* ctx, int64_t polls);
 /* Overwrite a device buffer (bytes, multiple of 8) on the context's stream;
  * benchmarks use it to evict the L2 cache between timed steps. */
 int emu_flush_l2(emu_context* ctx, void* device_buffer, int64_t bytes);
-/* One device-resident step (as emu_evolve_steps(ctx, 1)) launched kernel by
- * kernel with a CUDA event pair around each launch on the context stream.
+/* One device-resident step (as a step inside emu_evolve_steps(ctx, n > 1))
+ * launched kernel by kernel with a CUDA event pair around each launch on the
+ * context stream.
  * kernel_ms[i] receives the duration of kernel i in launch order (the RK
  * stages, with the mixed path's finalize kernel before each; stage 4 also
  * reduces compute_dt), then, when a re-sort follows the step, the whole
- * re-sort (keys, radix sort, gather) as one more entry; *nkernels their
- * count (at most 9).  Call after emu_evolve_begin. */
+ * re-sort (keys, radix sort, gather, and the deposit of the new state that
+ * stage 4 then leaves out, as emu_evolve_steps does) as one more entry;
+ * *nkernels their count (at most 9).  Call after emu_evolve_begin. */
 int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* nkernels);
 
 /* Plotfile (IO.cpp:11-38): mesh plotfile pltNNNNN plus, when
