@@ -1392,9 +1392,10 @@ __host__ __device__ constexpr int mixed_mesh_tile_offset()
            (mixed_mesh_tile<NF, WX, WY, WZ>() ? kMeshTileCells * Comb<NF>::NG * 4 : 0);
 }
 
-template <int NF, int WX, int WY, int WZ>
+// One kernel per RK stage SG (1-4): each holds only its stage's paths.
+template <int NF, int WX, int WY, int WZ, int SG>
 // (1D: 5 CTAs per SM at 96 registers beat 4 at 128 despite the spills)
-__global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S, int s,
+__global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S,
                                                             const float* __restrict__ gmesh,
                                                             long long* __restrict__ qout,
                                                             const long long* __restrict__ qdt,
@@ -1404,6 +1405,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     using H = Herm<NF>;
     using SWt = SW<WX, WY, WZ>;
     constexpr int NH = NF * NF, NS = 2 * NH;
+    constexpr int s = SG;
     constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
     // without the register preload, the CTA's slices of f0, k32 and ksum32
     // are staged in shared memory by bulk copies (the record area of the
@@ -2187,9 +2189,14 @@ void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, cons
 {
     EMU_W_DISPATCH(P, {
         constexpr int bytes = mixed_stage_smem_bytes<NF, WXv, WYv, WZv>();
-        smem_optin(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, bytes);
-        launch_pdl(k_rk4_stage_mixed<NF, WXv, WYv, WZv>, grid_for(S.n), kBlock, bytes, st, P, S, s, gmesh, qout, qdt,
-                   qm4, ctl, dt_mode);
+        auto go = [&](auto kern) {
+            smem_optin(kern, bytes);
+            launch_pdl(kern, grid_for(S.n), kBlock, bytes, st, P, S, gmesh, qout, qdt, qm4, ctl, dt_mode);
+        };
+        if (s == 1) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 1>);
+        else if (s == 2) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 2>);
+        else if (s == 3) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 3>);
+        else go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 4>);
     });
 }
 
