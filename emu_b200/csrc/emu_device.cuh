@@ -603,7 +603,8 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
 // barrier is needed, the records are only read).  The record holds the
 // value of slot c at SP + voff(c): the particle's f N in the full layout,
 // the values after the NV combinations in the combined one.  Eight threads
-// per record stream (BLOCK / 8 streams of NTILE / (BLOCK / 8) records): the
+// per record stream (BLOCK / 8 streams of NTILE / (BLOCK / 8) records), or
+// for 27-cell stencils a warp per stream with a lane per stencil cell: the
 // grouping of the FP32 run sums, and so the int64 results, do not depend on
 // which layout the records have.
 template <int NF, int BLOCK, int NTILE, class SWt, class T, class Conv>
@@ -616,6 +617,60 @@ __device__ __forceinline__ void tile_deposit_diag(const DevParams& P, T* diag, c
     constexpr int NSTREAM = BLOCK / kDiagSlots;
     constexpr int CH = (NTILE + NSTREAM - 1) / NSTREAM;
     static_assert(2 * NF <= kDiagSlots, "diagonal slots");
+    if constexpr (S == 27) {
+        // 27-cell stencils: lane k of a record stream (one warp) owns stencil
+        // cell k and sums all 2 NF values there: one weight load per record
+        // and lane, one cell index per flush
+        constexpr int NW = BLOCK / 32, CW = (NTILE + NW - 1) / NW;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (w >= NW || lane >= S) return;   // no block-wide barrier follows inside
+        const int kk = lane / 9, jj = (lane / 3) % 3, ii = lane % 3;
+        const bool on = SWt::on(P, ii, jj, kk);
+        float2 acc[NF];
+        auto flush = [&](int key) {
+            if (!on) return;
+            const int bx = key % P.n[0];
+            const int by = (key / P.n[0]) % P.n[1];
+            const int bz = key / (P.n[0] * P.n[1]);
+            T* g = diag + cell_of(P, bx, by, bz, ii, jj, kk) * kDiagSlots;
+#pragma unroll
+            for (int m = 0; m < NF; m++) {
+                atomic_add_mesh(g + 2 * m, conv(acc[m].x, (2 * m) / NF));
+                atomic_add_mesh(g + 2 * m + 1, conv(acc[m].y, (2 * m + 1) / NF));
+            }
+        };
+        const int r1 = min((w + 1) * CW, ntile);
+        int cur = -1;
+#pragma unroll
+        for (int m = 0; m < NF; m++) acc[m] = f2(0.f, 0.f);
+        for (int r = w * CW; r < r1; r++) {
+            const int key = skey[r];
+            if (key != cur) {
+                if (cur >= 0) flush(cur);
+#pragma unroll
+                for (int m = 0; m < NF; m++) acc[m] = f2(0.f, 0.f);
+                cur = key;
+            }
+            if (key < 0) continue;
+            const float* rec = srec + r * RW;
+            const float wt = rec[lane];
+            const float2 ww = f2(wt, wt);
+#pragma unroll
+            for (int m = 0; m < NF; m++) {
+                float2 x;
+                if (comb_layout) {
+                    x = reinterpret_cast<const float2*>(rec + SP + Comb<NF>::NV)[m];
+                } else {
+                    const int c0 = 2 * m, c1 = 2 * m + 1;
+                    x = f2(rec[SP + (c0 / NF) * NH + H::re(c0 % NF, c0 % NF)],
+                           rec[SP + (c1 / NF) * NH + H::re(c1 % NF, c1 % NF)]);
+                }
+                acc[m] = __ffma2_rn(x, ww, acc[m]);
+            }
+        }
+        if (cur >= 0) flush(cur);
+        return;
+    }
     const int c = threadIdx.x % kDiagSlots;
     const int stream = threadIdx.x / kDiagSlots;
     if (stream >= NSTREAM || c >= 2 * NF) return;   // no block-wide barrier follows inside
