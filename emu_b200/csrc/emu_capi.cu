@@ -447,7 +447,7 @@ int resort(emu_context* ctx, bool deposit = false)
         else r = emu_ctx::reduce_mesh(ctx, ctx->mesh[0], false, ctx->stream);
         if (r) return r;
     } else {
-        emu::launch_gather_state(ctx->nf, ctx->mixed, src, dst, ctx->idx2, ctx->stream);
+        emu::launch_gather_state(ctx->nf, ctx->mixed, ctx->P, src, dst, ctx->idx2, ctx->stream);
     }
     if ((r = check_launch(ctx, "resort"))) return r;
     ctx->cur = 1 - ctx->cur;

@@ -143,7 +143,7 @@ void launch_state_keys(const DevParams& P, const DevState& S, unsigned* keys, un
 // qmesh (mixed int64); the target must be zeroed
 void launch_gather_deposit(int nf, bool mixed, const DevParams& P, const DevState& src, const DevState& dst,
                            const unsigned* perm, double* mesh, long long* qmesh, cudaStream_t st);
-void launch_gather_state(int nf, bool mixed, const DevState& src, const DevState& dst, const unsigned* perm,
-                         cudaStream_t st);
+void launch_gather_state(int nf, bool mixed, const DevParams& P, const DevState& src, const DevState& dst,
+                         const unsigned* perm, cudaStream_t st);
 
 }  // namespace emu
