@@ -68,7 +68,7 @@ void launch_state_keys(const DevParams& P, const DevState& S, unsigned* keys, un
 void launch_gather_state(int nf, bool mixed, const DevParams& P, const DevState& src, const DevState& dst,
                          const unsigned* perm, cudaStream_t st)
 {
-    EMU_NF_DISPATCH(nf, (k_gather_state<NFv><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, mixed ? 1 : 0, P.c4)));
+    EMU_NF_DISPATCH(nf, (k_gather_state<NFv><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, mixed ? 1 : 0)));
 }
 
 void launch_gather_deposit(int nf, bool mixed, const DevParams& P, const DevState& src, const DevState& dst,

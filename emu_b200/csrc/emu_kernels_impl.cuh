@@ -1835,40 +1835,26 @@ __global__ void k_cell_keys_soa(DevParams P, DevState S, unsigned* keys, unsigne
 }
 
 template <int NF>
-// The fields derived from the momentum and N (vhat = pup/pupt and vscale =
-// c^4/(2 pupt) as k_pack computes them, the mixed path's FP32 copies) are
-// recomputed from the gathered values, not gathered: the same bits for less
-// of the HBM traffic.
-__global__ void k_gather_state(DevState src, DevState dst, const unsigned* __restrict__ perm, int mixed, double c4)
+// (a plain copy of every field: recomputing the derived ones from the
+// momentum instead measured no faster, and slower in isolation)
+__global__ void k_gather_state(DevState src, DevState dst, const unsigned* __restrict__ perm, int mixed)
 {
     constexpr int NS = 2 * NF * NF;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= src.n) return;
     const long long j = perm[i];
     dst.rslot[i] = (int)(i % kBlock);   // re-sorted: the identity rank
-    for (int d = 0; d < 3; d++) dst.pos[d][i] = src.pos[d][j];
+    for (int d = 0; d < 3; d++) { dst.pos[d][i] = src.pos[d][j]; dst.vhat[d][i] = src.vhat[d][j]; }
     dst.time[i] = src.time[j];
-    double pu[4];
-    for (int d = 0; d < 4; d++) {
-        pu[d] = src.pup[d][j];
-        dst.pup[d][i] = pu[d];
-    }
-    double nn[2];
-    for (int sp = 0; sp < 2; sp++) {
-        nn[sp] = src.Nn[sp][j];
-        dst.Nn[sp][i] = nn[sp];
-        dst.Ll[sp][i] = src.Ll[sp][j];
-    }
+    for (int d = 0; d < 4; d++) dst.pup[d][i] = src.pup[d][j];
+    for (int sp = 0; sp < 2; sp++) { dst.Nn[sp][i] = src.Nn[sp][j]; dst.Ll[sp][i] = src.Ll[sp][j]; }
+    dst.vscale[i] = src.vscale[j];
     dst.id[i] = src.id[j];
     for (int c = 0; c < NS; c++) dst.f0[c * dst.cap + i] = src.f0[c * src.cap + j];
-    dst.vscale[i] = c4 / (2. * pu[3]);
-    for (int d = 0; d < 3; d++) {
-        const double v = pu[d] / pu[3];
-        dst.vhat[d][i] = v;
-        if (mixed) dst.vhat32[d][i] = (float)v;
+    if (mixed) {
+        for (int d = 0; d < 3; d++) dst.vhat32[d][i] = src.vhat32[d][j];
+        for (int sp = 0; sp < 2; sp++) dst.N32[sp][i] = src.N32[sp][j];
     }
-    if (mixed)
-        for (int sp = 0; sp < 2; sp++) dst.N32[sp][i] = (float)nn[sp];
 }
 
 // Re-sort gather fused with the deposit of the gathered (new, cell-sorted)
@@ -2168,7 +2154,7 @@ void launch_gather_deposit_t(bool mixed, const DevParams& P, const DevState& src
         if (mixed) {
             // (mixed: the gather and the deposit as two kernels, each at its
             // own occupancy)
-            k_gather_state<NF><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, 1, P.c4);
+            k_gather_state<NF><<<grid_for(src.n), kBlock, 0, st>>>(src, dst, perm, 1);
             constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>();
             smem_optin(k_deposit_comb<NF, WXv, WYv, WZv>, bytes);
             k_deposit_comb<NF, WXv, WYv, WZv><<<grid_for(src.n), kBlock, bytes, st>>>(P, dst, qmesh);
