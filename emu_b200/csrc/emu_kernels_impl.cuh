@@ -15,8 +15,8 @@
 //   k_rk4_step_coop*         a whole step in one cooperative launch
 //   k_gather_deposit         re-sort gather + deposit of the new state
 //   k_rk4_stage_mixed<NF,W>  the same with FP32 interpolation and
-//                            self-interaction commutator, FP64 vacuum+matter
-//                            commutator and state, int64 fixed-point deposit
+//                            commutator (self-interaction + vacuum + matter),
+//                            FP64 state, int64 fixed-point deposit
 //   k_finalize_mixed<NF>     int64 mesh -> FP32 potential mesh
 //   k_dt<NF>                 compute_dt reduction (host-driven calls)
 //   k_deposit / k_rhs / k_stage_state / k_combine: unfused building blocks
@@ -1631,19 +1631,33 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 hsn[e] = (sp == 0 || H::is_im(e)) ? hs[e] : -hs[e];
                 f32[e] = (float)f[e];
             }
-            commutator<NF, float>(hsn, f32, ksi, ih);
-            // FP64 vacuum + matter part
-            double Hv[NH], Kv[NH];
+            {
+                // the vacuum + matter Hamiltonian, formed in FP64 with its
+                // trace removed (the commutator does not see the trace, and
+                // the diagonal differences keep their precision when
+                // rounded), joins the self-interaction part: one FP32
+                // commutator per species gives the RHS, which is FP32 (k32,
+                // ksum32) while the state and its accumulation stay FP64
+                double hv[NH];
 #pragma unroll
-            for (int e = 0; e < NH; e++) Hv[e] = P.M2[sp][e] * vs;
-            Hv[0] += sp == 0 ? mat : -mat;
-            commutator<NF, double>(Hv, f, Kv, P.inv_hbar);
+                for (int e = 0; e < NH; e++) hv[e] = P.M2[sp][e] * vs;
+                hv[0] += sp == 0 ? mat : -mat;
+                double tr = 0.0;
+#pragma unroll
+                for (int i = 0; i < NF; i++) tr += hv[H::re(i, i)];
+                tr *= 1.0 / NF;
+#pragma unroll
+                for (int i = 0; i < NF; i++) hv[H::re(i, i)] -= tr;
+#pragma unroll
+                for (int e = 0; e < NH; e++) hsn[e] += (float)hv[e];
+            }
+            commutator<NF, float>(hsn, f32, ksi, ih);
             double fn[NH];
             if (s < 4) {
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
                     const long long o = (sp * NH + e) * cap + p;
-                    const float kc = (float)(Kv[e] + (double)ksi[e]);
+                    const float kc = ksi[e];
                     float ks;
                     if constexpr (PRELOAD) ks = ksa[sp * NH + e];
                     else ks = s > 1 ? sks[(sp * NH + e) * kBlock + t] : 0.f;
@@ -1657,7 +1671,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     float ks;
                     if constexpr (PRELOAD) ks = ksa[sp * NH + e];
                     else ks = sks[(sp * NH + e) * kBlock + t];
-                    fn[e] = y0[e] + w6 * ((double)ks + (Kv[e] + (double)ksi[e]));
+                    fn[e] = y0[e] + w6 * ((double)ks + (double)ksi[e]);
                 }
                 stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : s4[(5 + sp) * kBlock + t], P.maxError);
 #pragma unroll

@@ -48,9 +48,9 @@ extern "C" {
 
 /* arithmetic of the path */
 #define EMU_PREC_FP64    0     /* FP64 throughout (the reference's PRECISION=DOUBLE) */
-#define EMU_PREC_MIXED   1     /* FP32 interpolation/potentials/commutator, int64
-                                  fixed-point deposit, FP64 rho accumulation,
-                                  renormalisation and vacuum+matter term */
+#define EMU_PREC_MIXED   1     /* FP32 interpolation/potentials/commutator (the
+                                  RHS), int64 fixed-point deposit, FP64 rho
+                                  accumulation and renormalisation */
 
 /*
  * Run parameters.  Mirrors TestParams (Source/Parameters.H:11-132) in the

@@ -1,5 +1,5 @@
-"""Mixed-precision path (FP32 interpolation / self-interaction commutator,
-int64 fixed-point deposit, FP64 state, vacuum+matter term and
+"""Mixed-precision path (FP32 interpolation and commutator, i.e. an FP32
+right-hand side, int64 fixed-point deposit, FP64 state accumulation and
 renormalisation) against the FP64 oracle.
 
 Stated tolerances:
