@@ -1595,8 +1595,8 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         }
         const float ih = (float)P.inv_hbar;
         const double mat = P.sqrt2GF_inv_vol * P.matter;
-        const double aw = s > 1 ? dt * kRK4A[s - 1] : 0.0;
-        const double an = s < 4 ? dt * kRK4A[s] : 0.0;
+        const float awf = (float)(s > 1 ? dt * kRK4A[s - 1] : 0.0);
+        const float anf = (float)(s < 4 ? dt * kRK4A[s] : 0.0);
         const double w6 = dt * (1.0 / 6.0);
         int stt = 0;
         if constexpr (STAGE) {
@@ -1611,7 +1611,11 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
 #pragma unroll
         for (int sp = 0; sp < 2; sp++) {
             if (!live) break;
-            double y0[NH], f[NH];
+            // the stage state Y_s = y0 + aw K_{s-1} only enters the FP32
+            // commutator and (stages 1-3) the FP32 deposit: formed in FP32
+            // from the FP64 step-start state; stage 4's update below is FP64
+            double y0[NH];
+            float y0f[NH], f32[NH];
 #pragma unroll
             for (int e = 0; e < NH; e++) {
                 float k;
@@ -1622,15 +1626,13 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     y0[e] = sf0[(sp * NH + e) * kBlock + t];
                     k = s > 1 ? sk[(sp * NH + e) * kBlock + t] : 0.f;
                 }
-                f[e] = s > 1 ? y0[e] + aw * (double)k : y0[e];
+                y0f[e] = (float)y0[e];
+                f32[e] = s > 1 ? fmaf(awf, k, y0f[e]) : y0f[e];
             }
             // nubar: H_SI conjugated and negated (generate_code.py:317-355)
-            float hsn[NH], f32[NH], ksi[NH];
+            float hsn[NH], ksi[NH];
 #pragma unroll
-            for (int e = 0; e < NH; e++) {
-                hsn[e] = (sp == 0 || H::is_im(e)) ? hs[e] : -hs[e];
-                f32[e] = (float)f[e];
-            }
+            for (int e = 0; e < NH; e++) hsn[e] = (sp == 0 || H::is_im(e)) ? hs[e] : -hs[e];
             {
                 // the vacuum + matter Hamiltonian, formed in FP64 with its
                 // trace removed (the commutator does not see the trace, and
@@ -1652,7 +1654,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 for (int e = 0; e < NH; e++) hsn[e] += (float)hv[e];
             }
             commutator<NF, float>(hsn, f32, ksi, ih);
-            double fn[NH];
+            const float Ns = Nsp[sp];
             if (s < 4) {
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
@@ -1663,9 +1665,11 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     else ks = s > 1 ? sks[(sp * NH + e) * kBlock + t] : 0.f;
                     S.k32[o] = kc;
                     S.ksum32[o] = (s == 1) ? kc : fmaf(2.f, kc, ks);
-                    fn[e] = y0[e] + an * (double)kc;
+                    // the next stage's state, for the deposit only
+                    fN[sp * NH + e] = fmaf(anf, kc, y0f[e]) * Ns;
                 }
             } else {
+                double fn[NH];
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
                     float ks;
@@ -1675,11 +1679,11 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 }
                 stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : s4[(5 + sp) * kBlock + t], P.maxError);
 #pragma unroll
-                for (int e = 0; e < NH; e++) S.f0[(sp * NH + e) * cap + p] = fn[e];
+                for (int e = 0; e < NH; e++) {
+                    S.f0[(sp * NH + e) * cap + p] = fn[e];
+                    fN[sp * NH + e] = (float)fn[e] * Ns;
+                }
             }
-            const float Ns = Nsp[sp];
-#pragma unroll
-            for (int e = 0; e < NH; e++) fN[sp * NH + e] = (float)fn[e] * Ns;
         }
         if (s == 4 && live) {
             double xn[3] = {x, y, z};
