@@ -566,13 +566,22 @@ def run_emu(args):
         "cpu_baseline": cpu,
         # per step: the step kernels (+ the L2 flush for small states); per
         # re-sort: keys, radix sort (histogram, scan, one pass per 8 key
-        # bits), gather
+        # bits), gather (+ the mixed path's deposit of the sorted state); per
+        # emu_evolve_steps call of the mixed path: the stage-4 mesh control
         "gpu_launches": args.steps * kernels_per_step + (args.steps if flush is not None else 0) +
-                        resorts * (4 + (key_bits + 7) // 8),
+                        resorts * (4 + (key_bits + 7) // 8 + (1 if mixed else 0)) +
+                        ((args.steps if flush is not None else 1) if mixed else 0),
         "clocks": clocks,
         "wall_s": wall,
         "kernel_ms_per_step": [float(x) for x in per_kernel],
     }
+    if mixed:
+        out["path"] = ("mixed precision: FP32 interpolation and right-hand side (one FP32 commutator per species, "
+                       "the vacuum + matter Hamiltonian rounded in), FP64 state accumulation and renormalisation, "
+                       "int64 fixed-point deposits in the combined self-interaction layout; inside one "
+                       "emu_evolve_steps call the stage-4 mesh keeps the combined layout and the diagonal N_ii "
+                       "that compute_dt reads, and the call's last step deposits it in full (the mesh a caller "
+                       "reads); results do not depend on how a run is split into calls")
     if args.workload == "c4" and ws == 1:
         out["adjoint"] = run_adjoint(ctx, recs, p, stream, ms_per_step, int(p.nsteps), 25)
     elif args.adjoint and ws == 1 and not multi:
