@@ -213,11 +213,28 @@ int key_bits(long long ncells)
 }
 
 // device radix sort of (keys, idx) -> idx2 holds the permutation
-int sort_perm(emu_context* ctx, long long n)
+int sort_perm(emu_context* ctx, long long n, cudaStream_t st)
 {
     size_t tb = ctx->sort_tmp_bytes;
     CU(cub::DeviceRadixSort::SortPairs(ctx->sort_tmp, tb, ctx->keys, ctx->keys2, ctx->idx, ctx->idx2, (int)n, 0,
-                                       key_bits(ctx->P.ncells), ctx->stream));
+                                       key_bits(ctx->P.ncells), st));
+    return EMU_OK;
+}
+int sort_perm(emu_context* ctx, long long n) { return sort_perm(ctx, n, ctx->stream); }
+
+// The mixed path's re-sort after a step, around stage 4: keys of the
+// positions after the step and their sort before it (the inverse
+// permutation in idx), the deposit of the re-sorted state after it.  The
+// next step's first mesh is zeroed here too: once the run has ended the
+// finalize kernel does not, and the unchanged state is deposited again.
+int enqueue_sc_before(emu_context* ctx, cudaStream_t st)
+{
+    const DevState& S = ctx->S[ctx->cur];
+    CU(cudaMemsetAsync(ctx->qmesh[0], 0, sizeof(long long) * ctx->P.ncells * ctx->ND, st));
+    emu::launch_sc_keys(ctx->P, S, ctx->ctl, ctx->keys, ctx->idx, st);
+    int r;
+    if ((r = sort_perm(ctx, S.n, st))) return r;
+    emu::launch_sc_invert(ctx->idx2, ctx->idx, S.n, st);
     return EMU_OK;
 }
 
@@ -357,10 +374,22 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt, bool dep4
         const bool comb = s != 4 || ctx->P.m4_reduced;
         emu::launch_finalize_mixed(ctx->nf, ctx->P, ctx->qmesh[a], ctx->qmesh[b], ctx->gmesh, ctx->ctl, comb,
                                    (s == 3 && ctx->P.m4_reduced) ? m4_target(ctx) : nullptr, st);
+        int r;
+        if (s == 4 && !dep4) {
+            // the re-sort that follows, made by stage 4's stores (see
+            // enqueue_sc_before), then the deposit of the re-sorted state
+            DevState& D = ctx->S[1 - ctx->cur];
+            D.n = S.n;
+            if ((r = enqueue_sc_before(ctx, st))) return r;
+            emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, 4, ctx->gmesh, nullptr, ctx->qmesh[1], m4_target(ctx),
+                                        ctx->ctl, with_dt ? emu::DT_ADVANCE : -1, st, &D, ctx->idx);
+            emu::launch_deposit_comb(ctx->nf, ctx->P, D, ctx->qmesh[0], st);
+            if ((r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[0], true, st))) return r;
+            continue;
+        }
         const bool dep = s < 4 || dep4;
         emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr, ctx->qmesh[1],
                                     m4_target(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
-        int r;
         if (dep && (r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return r;
         a = b;
     }
@@ -428,6 +457,13 @@ int step_generic(emu_context* ctx, double dt)
 // mesh instead (mesh[0] / qmesh[0], zeroed here first)
 int resort(emu_context* ctx, bool deposit = false)
 {
+    if (deposit && ctx->mixed) {
+        // (the step's stage 4 has made it, into the other buffer)
+        ctx->cur = 1 - ctx->cur;
+        ctx->steps_since_sort = 0;
+        ctx->adj_valid = false;
+        return EMU_OK;
+    }
     DevState& src = ctx->S[ctx->cur];
     DevState& dst = ctx->S[1 - ctx->cur];
     dst.n = src.n;
@@ -486,6 +522,7 @@ int build_graph(emu_context* ctx, int variant)
     ctx->graph[ctx->cur][variant] = ex;
     ctx->graph_P[ctx->cur][variant] = ctx->P;
     ctx->graph_S[ctx->cur][variant] = ctx->S[ctx->cur];
+    ctx->graph_D[ctx->cur][variant] = ctx->S[1 - ctx->cur];
     return EMU_OK;
 }
 
@@ -515,7 +552,8 @@ int emu_ctx::step_device(emu_context* ctx, bool last_stage_deposit)
         // the parameters or the particle arrays changed since (a reload of
         // a different set); a reload of an equal set reuses it
         if (ctx->graph[c][v] && (std::memcmp(&ctx->graph_P[c][v], &ctx->P, sizeof(DevParams)) != 0 ||
-                                 std::memcmp(&ctx->graph_S[c][v], &ctx->S[c], sizeof(DevState)) != 0)) {
+                                 std::memcmp(&ctx->graph_S[c][v], &ctx->S[c], sizeof(DevState)) != 0 ||
+                                 std::memcmp(&ctx->graph_D[c][v], &ctx->S[1 - c], sizeof(DevState)) != 0)) {
             cudaGraphExecDestroy(ctx->graph[c][v]);
             ctx->graph[c][v] = nullptr;
         }
@@ -1038,12 +1076,15 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
     const bool resort_due = ctx->prm.resort_interval > 0 && ctx->steps_since_sort + 1 >= ctx->prm.resort_interval;
     if (max_kernels < nk + (resort_due ? 1 : 0))
         return fail(ctx, EMU_ERR_ARG, "emu_profile_step: kernel_ms too small");
-    std::vector<cudaEvent_t> ev(2 * nk + 2);
+    std::vector<cudaEvent_t> ev(2 * nk + 4);
     for (auto& e : ev) CU(cudaEventCreate(&e));
     const DevState& S = ctx->S[ctx->cur];
     cudaStream_t st = ctx->stream;
     int k = 0;
     auto rec = [&](int i) { return cudaEventRecord(ev[i], st); };
+    // (mixed: the re-sort made around stage 4, timed as one entry after the
+    // stages: its keys and sort before stage 4 plus its deposit after it)
+    const bool sc = ctx->mixed && resort_due;
     if (ctx->mixed) {
         int a = 0;
         for (int s = 1; s <= 4; s++) {
@@ -1054,15 +1095,30 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
                                        (s == 3 && ctx->P.m4_reduced) ? m4_target(ctx) : nullptr, st);
             rec(2 * k + 1);
             k++;
-            // as in the evolve loop: a re-sort that follows makes the
-            // deposit of the new state instead of stage 4
+            int rr;
+            if (s == 4 && sc) {
+                DevState& D = ctx->S[1 - ctx->cur];
+                D.n = S.n;
+                rec(2 * nk);
+                if ((rr = enqueue_sc_before(ctx, st))) return rr;
+                rec(2 * nk + 1);
+                rec(2 * k);
+                emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, 4, ctx->gmesh, nullptr, ctx->qmesh[1],
+                                            m4_target(ctx), ctx->ctl, emu::DT_ADVANCE, st, &D, ctx->idx);
+                rec(2 * k + 1);
+                k++;
+                rec(2 * nk + 2);
+                emu::launch_deposit_comb(ctx->nf, ctx->P, D, ctx->qmesh[0], st);
+                if ((rr = emu_ctx::reduce_mesh(ctx, ctx->qmesh[0], true, st))) return rr;
+                rec(2 * nk + 3);
+                continue;
+            }
             const bool dep = s < 4 || !resort_due;
             rec(2 * k);
             emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr,
                                         ctx->qmesh[1], m4_target(ctx), ctx->ctl, s == 4 ? emu::DT_ADVANCE : -1, st);
             rec(2 * k + 1);
             k++;
-            int rr;
             if (dep && (rr = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return rr;
             a = b;
         }
@@ -1084,7 +1140,9 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
     if (ctx->mixed && (r = sum_full_parts(ctx))) return r;
     ctx->cur_mesh = ctx->mixed ? 1 : 3;
     if (ctx->prm.resort_interval > 0) ctx->steps_since_sort++;
-    if (resort_due) {
+    if (sc) {
+        if ((r = resort(ctx, true))) return r;   // (the buffers change places)
+    } else if (resort_due) {
         // the re-sort that follows the step (keys, radix sort, gather and
         // the deposit of the new state) as one more entry
         rec(2 * k);
@@ -1094,6 +1152,12 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
     }
     CU(cudaStreamSynchronize(st));
     for (int i = 0; i < k; i++) CU(cudaEventElapsedTime(&kernel_ms[i], ev[2 * i], ev[2 * i + 1]));
+    if (sc) {
+        float a = 0.f, b = 0.f;
+        CU(cudaEventElapsedTime(&a, ev[2 * nk], ev[2 * nk + 1]));
+        CU(cudaEventElapsedTime(&b, ev[2 * nk + 2], ev[2 * nk + 3]));
+        kernel_ms[k++] = a + b;
+    }
     for (auto& e : ev) cudaEventDestroy(e);
     *nkernels = k;
     return EMU_OK;

@@ -58,6 +58,7 @@ struct emu_context {
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     DevParams graph_P[2][2];            // kernel arguments each graph was captured with
     DevState graph_S[2][2];
+    DevState graph_D[2][2];             // and the other buffer (the mixed stage 4 re-sorts into it)
     int steps_since_sort = 0;
     bool coop = false;                  // whole-step cooperative kernel (small FP64 problems)
     emu_adjoint* adj = nullptr;         // allocated by the first adjoint call

@@ -15,7 +15,8 @@ namespace emu {
                                           double*, cudaStream_t);                                                \
     extern template void launch_rk4_stage_mixed_t<NF>(const DevParams&, const DevState&, int, const float*,      \
                                                       long long*, const long long*, long long*, StepCtl*, int,   \
-                                                      cudaStream_t);                                             \
+                                                      cudaStream_t, const DevState*, const unsigned*);           \
+    extern template void launch_deposit_comb_t<NF>(const DevParams&, const DevState&, long long*, cudaStream_t);  \
     extern template void launch_deposit_q_t<NF>(const DevParams&, const DevState&, const double*, long long*,    \
                                                 cudaStream_t);                                                   \
     extern template bool coop_step_fits_t<NF>(const DevParams&, long long);                                      \
@@ -131,10 +132,27 @@ cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, 
 
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
                             long long* qmesh_out, const long long* qmesh_dt, long long* qmesh_m4, StepCtl* ctl,
-                            int dt_mode, cudaStream_t st)
+                            int dt_mode, cudaStream_t st, const DevState* D, const unsigned* inv)
 {
-    if (nf == 2) launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st);
-    else launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st);
+    if (nf == 2) launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st, D, inv);
+    else launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st, D, inv);
+}
+
+void launch_deposit_comb(int nf, const DevParams& P, const DevState& S, long long* qmesh, cudaStream_t st)
+{
+    if (nf == 2) launch_deposit_comb_t<2>(P, S, qmesh, st);
+    else launch_deposit_comb_t<3>(P, S, qmesh, st);
+}
+
+void launch_sc_keys(const DevParams& P, const DevState& S, const StepCtl* ctl, unsigned* keys, unsigned* idx,
+                    cudaStream_t st)
+{
+    k_sc_keys<<<grid_for(S.n), kBlock, 0, st>>>(P, S, ctl, keys, idx);
+}
+
+void launch_sc_invert(const unsigned* perm, unsigned* inv, long long n, cudaStream_t st)
+{
+    k_sc_invert<<<grid_for(n), kBlock, 0, st>>>(perm, inv, n);
 }
 
 static unsigned reduce_grid(long long ncells)

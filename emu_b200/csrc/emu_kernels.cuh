@@ -110,9 +110,22 @@ bool coop_step_fits(int nf, const DevParams& P, long long n);
 cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, double* const mesh[4], long long nmesh,
                                  StepCtl* ctl, int dt_mode, cudaStream_t st);
 // qmesh_m4: stage 3's target for the full stage-4 mesh (DevParams::m4_reduced)
+// D, inv (stage 4 only): the stage that makes the cell re-sort following the
+// step: particle p's new state and unchanged fields go to slot inv[p] of D
+// (launch_sc_keys, the radix sort and launch_sc_invert before it; the
+// combined deposit of D, launch_deposit_comb, after it).
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
                             long long* qmesh_out, const long long* qmesh_dt, long long* qmesh_m4, StepCtl* ctl,
-                            int dt_mode, cudaStream_t st);
+                            int dt_mode, cudaStream_t st, const DevState* D = nullptr,
+                            const unsigned* inv = nullptr);
+// the combined deposit of a cell-sorted mixed state into qmesh (zeroed)
+void launch_deposit_comb(int nf, const DevParams& P, const DevState& S, long long* qmesh, cudaStream_t st);
+// keys of the positions after the step (the stage-4 push; unchanged once the
+// run has ended) and the identity index
+void launch_sc_keys(const DevParams& P, const DevState& S, const StepCtl* ctl, unsigned* keys, unsigned* idx,
+                    cudaStream_t st);
+// inv[perm[i]] = i
+void launch_sc_invert(const unsigned* perm, unsigned* inv, long long n, cudaStream_t st);
 // comb: qread holds the combined layout (else the full mesh).  qzero is
 // zeroed with its diagonal slots (ncells * (8 NF^2 + kDiagSlots)); qzero_m4
 // (before stage 3, or nullptr) on the steps that deposit the full stage-4

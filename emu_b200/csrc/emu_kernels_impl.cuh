@@ -119,6 +119,24 @@ __device__ __forceinline__ double wrap_coord(double x, double L)
     return x;
 }
 
+// the stage-4 particle push: x += sum_i dt b_i c p/p^t, t += sum_i dt b_i,
+// then the periodic wrap (one definition for the mixed stage 4 and for the
+// keys of the re-sort computed before it, so that both give the same bits)
+__device__ __forceinline__ void rk4_push(const DevParams& P, double dt, const double* pq, double* xn, double& tn)
+{
+    const double ipt = 1.0 / pq[3];
+    const double kxv[3] = {pq[0] * ipt * kC, pq[1] * ipt * kC, pq[2] * ipt * kC};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const double w = dt * kRK4B[i];
+#pragma unroll
+        for (int d = 0; d < 3; d++) xn[d] = __dadd_rn(__dmul_rn(w, kxv[d]), xn[d]);
+        tn = __dadd_rn(w, tn);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) xn[d] = wrap_coord(xn[d], P.L[d]);
+}
+
 __device__ __forceinline__ void report_bad(StepCtl* ctl, int st, long long id)
 {
     if (st) {
@@ -1391,15 +1409,73 @@ __host__ __device__ constexpr int mixed_mesh_tile_offset()
            (mixed_mesh_tile<NF, WX, WY, WZ>() ? kMeshTileCells * Comb<NF>::NG * 4 : 0);
 }
 
+// Keys of the cell re-sort that the next stage 4 scatters into: every
+// particle's stencil key after the step (the stage-4 push; none once the
+// run has ended), with the identity index, for the radix sort.
+__global__ void k_sc_keys(DevParams P, DevState S, const StepCtl* __restrict__ ctl, unsigned* __restrict__ keys,
+                          unsigned* __restrict__ idx)
+{
+    const int done = __ldcg(&ctl->done);
+    const double dt = __ldcg(&ctl->dt);
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.n) return;
+    double xn[3] = {S.pos[0][p], S.pos[1][p], S.pos[2][p]};
+    if (!done) {
+        const double pq[4] = {S.pup[0][p], S.pup[1][p], S.pup[2][p], S.pup[3][p]};
+        double tn = 0.0;
+        rk4_push(P, dt, pq, xn, tn);
+    }
+    Stencil<double> st;
+    make_stencil<double>(P, xn[0], xn[1], xn[2], st);
+    keys[p] = (unsigned)stencil_key(P, st.b);
+    idx[p] = (unsigned)p;
+}
+
+// inverse of the sort's permutation: particle perm[i] goes to slot i
+__global__ void k_sc_invert(const unsigned* __restrict__ perm, unsigned* __restrict__ inv, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) inv[perm[i]] = (unsigned)i;
+}
+
+// the fields of particle p that no stage changes, into slot q of D
+__device__ __forceinline__ void sc_static_fields(const DevParams& P, const DevState& S, const DevState& D, long long p,
+                                                 long long q, const double* pq, const double* L2)
+{
+    D.rslot[q] = (int)(q % kBlock);   // in cell order: the identity rank
+    D.id[q] = S.id[p];
+#pragma unroll
+    for (int sp = 0; sp < 2; sp++) {
+        const double nn = S.Nn[sp][p];
+        D.Nn[sp][q] = nn;
+        D.N32[sp][q] = (float)nn;
+        D.Ll[sp][q] = L2[sp];
+    }
+#pragma unroll
+    for (int d = 0; d < 4; d++) D.pup[d][q] = pq[d];
+    D.vscale[q] = P.c4 / (2. * pq[3]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double v = pq[d] / pq[3];
+        D.vhat[d][q] = v;
+        D.vhat32[d][q] = (float)v;
+    }
+}
+
 // One kernel per RK stage SG (1-4): each holds only its stage's paths.
-template <int NF, int WX, int WY, int WZ, int SG>
+// SC (stage 4 before a re-sort): the new state and every unchanged field of
+// particle p go to slot inv[p] of D, the other particle buffer, in the new
+// cell order (the re-sort's gather, made by the stores of this stage; its
+// keys and sort ran before it, from the same push); D's deposit follows.
+template <int NF, int WX, int WY, int WZ, int SG, bool SC = false>
 // (1D: 5 CTAs per SM at 96 registers beat 4 at 128 despite the spills)
 __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S,
                                                             const float* __restrict__ gmesh,
                                                             long long* __restrict__ qout,
                                                             const long long* __restrict__ qdt,
                                                             long long* __restrict__ qm4, StepCtl* ctl,
-                                                            int dt_mode)
+                                                            int dt_mode, DevState D,
+                                                            const unsigned* __restrict__ inv)
 {
     using H = Herm<NF>;
     using SWt = SW<WX, WY, WZ>;
@@ -1412,9 +1488,28 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     constexpr bool STAGE = !PRELOAD;
     // (programmatic dependent launch: see grid_dep_wait; the finalize
     // kernel before this stage has waited for the previous stage)
+    static_assert(!SC || SG == 4, "the re-sort scatter is stage 4's");
     const int done = __ldcg(&ctl->done);
     const double dt = __ldcg(&ctl->dt);   // both control loads in one round trip
-    if (done) return;
+    if (done) {
+        if constexpr (SC) {
+            // after the run's end the re-sort still moves the unchanged
+            // state (its keys were those of the unchanged positions)
+            grid_dep_wait();
+            const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (p < S.n) {
+                const long long q = inv[p];
+                double pq[4], L2[2];
+                for (int d = 0; d < 4; d++) pq[d] = S.pup[d][p];
+                for (int sp = 0; sp < 2; sp++) L2[sp] = S.Ll[sp][p];
+                sc_static_fields(P, S, D, p, q, pq, L2);
+                for (int d = 0; d < 3; d++) D.pos[d][q] = S.pos[d][p];
+                D.time[q] = S.time[p];
+                for (int c = 0; c < 2 * NF * NF; c++) D.f0[c * D.cap + q] = S.f0[c * S.cap + p];
+            }
+        }
+        return;
+    }
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = p < S.n;
     const long long cap = S.cap;
@@ -1505,6 +1600,8 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     grid_dep_wait();
     grid_dep_launch();
     bool live = active;   // false: this particle's staged state never arrived
+    long long qsc = 0;    // SC: the particle's slot in D (the inverse, written before this stage)
+    if constexpr (SC) qsc = active ? (long long)inv[p] : 0;
     if constexpr (STAGE) {
         if (s > 1 && t < 32)
             for (int c = t; c < 2 * NS; c += 32) {
@@ -1680,7 +1777,8 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : s4[(5 + sp) * kBlock + t], P.maxError);
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
-                    S.f0[(sp * NH + e) * cap + p] = fn[e];
+                    if constexpr (SC) D.f0[(sp * NH + e) * cap + qsc] = fn[e];
+                    else S.f0[(sp * NH + e) * cap + p] = fn[e];
                     fN[sp * NH + e] = (float)fn[e] * Ns;
                 }
             }
@@ -1690,21 +1788,18 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
             double tn = PRELOAD ? t_in : s4[t];
             const double pq[4] = {PRELOAD ? pu[0] : s4[kBlock + t], PRELOAD ? pu[1] : s4[2 * kBlock + t],
                                   PRELOAD ? pu[2] : s4[3 * kBlock + t], PRELOAD ? pu[3] : s4[4 * kBlock + t]};
-            const double ipt = 1.0 / pq[3];
-            const double kxv[3] = {pq[0] * ipt * kC, pq[1] * ipt * kC, pq[2] * ipt * kC};
+            rk4_push(P, dt, pq, xn, tn);
+            if constexpr (SC) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const double w = dt * kRK4B[i];
+                for (int d = 0; d < 3; d++) D.pos[d][qsc] = xn[d];
+                D.time[qsc] = tn;
+                const double L2[2] = {PRELOAD ? Lsp[0] : s4[5 * kBlock + t], PRELOAD ? Lsp[1] : s4[6 * kBlock + t]};
+                sc_static_fields(P, S, D, p, qsc, pq, L2);
+            } else {
 #pragma unroll
-                for (int d = 0; d < 3; d++) xn[d] = __dadd_rn(__dmul_rn(w, kxv[d]), xn[d]);
-                tn = __dadd_rn(w, tn);
+                for (int d = 0; d < 3; d++) S.pos[d][p] = xn[d];
+                S.time[p] = tn;
             }
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                xn[d] = wrap_coord(xn[d], P.L[d]);
-                S.pos[d][p] = xn[d];
-            }
-            S.time[p] = tn;
             report_bad(ctl, stt, S.id[p]);
             make_stencil<float>(P, xn[0], xn[1], xn[2], st);
         }
@@ -2204,18 +2299,31 @@ void launch_rhs_t(const DevParams& P, const DevState& S, const double* f, const 
 
 template <int NF>
 void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, const float* gmesh, long long* qout,
-                              const long long* qdt, long long* qm4, StepCtl* ctl, int dt_mode, cudaStream_t st)
+                              const long long* qdt, long long* qm4, StepCtl* ctl, int dt_mode, cudaStream_t st,
+                              const DevState* D, const unsigned* inv)
 {
     EMU_W_DISPATCH(P, {
         constexpr int bytes = mixed_stage_smem_bytes<NF, WXv, WYv, WZv>();
+        const DevState& Dv = D ? *D : S;
         auto go = [&](auto kern) {
             smem_optin(kern, bytes);
-            launch_pdl(kern, grid_for(S.n), kBlock, bytes, st, P, S, gmesh, qout, qdt, qm4, ctl, dt_mode);
+            launch_pdl(kern, grid_for(S.n), kBlock, bytes, st, P, S, gmesh, qout, qdt, qm4, ctl, dt_mode, Dv, inv);
         };
         if (s == 1) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 1>);
         else if (s == 2) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 2>);
         else if (s == 3) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 3>);
+        else if (D) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 4, true>);
         else go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 4>);
+    });
+}
+
+template <int NF>
+void launch_deposit_comb_t(const DevParams& P, const DevState& S, long long* qmesh, cudaStream_t st)
+{
+    EMU_W_DISPATCH(P, {
+        constexpr int bytes = tile_smem_bytes<NF, SW<WXv, WYv, WZv>, float>();
+        smem_optin(k_deposit_comb<NF, WXv, WYv, WZv>, bytes);
+        k_deposit_comb<NF, WXv, WYv, WZv><<<grid_for(S.n), kBlock, bytes, st>>>(P, S, qmesh);
     });
 }
 
