@@ -566,8 +566,10 @@ def run_emu(args):
         "cpu_baseline": cpu,
         # per step: the step kernels (+ the L2 flush for small states); per
         # re-sort: keys, radix sort (histogram, scan, one pass per 8 key
-        # bits), gather (+ the mixed path's deposit of the sorted state); per
-        # emu_evolve_steps call of the mixed path: the stage-4 mesh control
+        # bits) and the gather (FP64), or the inversion of the permutation
+        # and the deposit of the sorted state (mixed: stage 4 stores in
+        # cell order); per emu_evolve_steps call of the mixed path: the
+        # stage-4 mesh control
         "gpu_launches": args.steps * kernels_per_step + (args.steps if flush is not None else 0) +
                         resorts * (4 + (key_bits + 7) // 8 + (1 if mixed else 0)) +
                         ((args.steps if flush is not None else 1) if mixed else 0),
