@@ -1528,14 +1528,17 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     float* const sks = sk + NS * kBlock;                             // [NS][kBlock]
     double* const s4 = reinterpret_cast<double*>(sks + NS * kBlock); // stage 4: time, pup[4], L[2] x kBlock
     const long long p0 = (long long)blockIdx.x * kBlock;
+    // slices of k32 and ksum32 staged: none in stage 1; K_1 alone in stage
+    // 2 (after stage 1 the running sum K_1 + 2 K_2 + ... is K_1 itself, so
+    // stage 1 stores no ksum32); both in stages 3 and 4
+    constexpr int NKS = s == 1 ? 0 : (s == 2 ? NS : 2 * NS);
     if constexpr (STAGE) {
         // f0 is written only by the previous step: its copies start before
         // the dependency wait, k32 and ksum32 (the previous stage's) after it
         if (t < 32) {
             if (t == 0) {
                 mbar_init(&stage_bar, 1);
-                mbar_expect_tx(&stage_bar, NS * kBlock * 8 + (s > 1 ? 2 * NS * kBlock * 4 : 0) +
-                                               (s == 4 ? 7 * kBlock * 8 : 0));
+                mbar_expect_tx(&stage_bar, NS * kBlock * 8 + NKS * kBlock * 4 + (s == 4 ? 7 * kBlock * 8 : 0));
                 if constexpr (MTILE) mbar_init(&mesh_bar, 1);
             }
             __syncwarp();
@@ -1604,7 +1607,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     if constexpr (SC) qsc = active ? (long long)inv[p] : 0;
     if constexpr (STAGE) {
         if (s > 1 && t < 32)
-            for (int c = t; c < 2 * NS; c += 32) {
+            for (int c = t; c < NKS; c += 32) {
                 const float* src = c < NS ? S.k32 + c * cap + p0 : S.ksum32 + (c - NS) * cap + p0;
                 bulk_g2s(sk + c * kBlock, src, kBlock * 4, &stage_bar);
             }
@@ -1653,7 +1656,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
 #pragma unroll
             for (int c = 0; c < NS; c++) {
                 ka[c] = s > 1 ? k32p[c * cap + p] : 0.f;
-                ksa[c] = s > 1 ? ks32p[c * cap + p] : 0.f;
+                ksa[c] = s > 2 ? ks32p[c * cap + p] : ka[c];   // (stage 2: the sum is K_1)
             }
         }
         // FP32 self-interaction part, trace removed (it commutes; three
@@ -1759,9 +1762,10 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     const float kc = ksi[e];
                     float ks;
                     if constexpr (PRELOAD) ks = ksa[sp * NH + e];
-                    else ks = s > 1 ? sks[(sp * NH + e) * kBlock + t] : 0.f;
+                    else ks = s > 2 ? sks[(sp * NH + e) * kBlock + t] : (s == 2 ? sk[(sp * NH + e) * kBlock + t] : 0.f);
                     S.k32[o] = kc;
-                    S.ksum32[o] = (s == 1) ? kc : fmaf(2.f, kc, ks);
+                    // (after stage 1 the running sum is K_1 = k32)
+                    if (s > 1) S.ksum32[o] = fmaf(2.f, kc, ks);
                     // the next stage's state, for the deposit only
                     fN[sp * NH + e] = fmaf(anf, kc, y0f[e]) * Ns;
                 }
