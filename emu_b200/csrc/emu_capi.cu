@@ -101,10 +101,10 @@ T* carve(char*& ptr, long long count)
     return r;
 }
 
-size_t persistent_bytes(int NS, bool mixed, long long cap)
+size_t persistent_bytes(int NS, bool mixed, bool f0copy, long long cap)
 {
     size_t per = (size_t)(16 + NS) * 8 + 8;
-    if (mixed) per += 5 * 4;
+    if (mixed) per += (size_t)(5 + (f0copy ? NS : 0)) * 4;
     return per * cap + 64 * 256;
 }
 
@@ -114,7 +114,7 @@ size_t transient_bytes(int NS, bool mixed, long long cap)
     return (size_t)2 * NS * 8 * cap + (size_t)4 * cap + 4 * 256;
 }
 
-void assign_persistent(DevState& S, void* block, int NS, bool mixed, long long cap)
+void assign_persistent(DevState& S, void* block, int NS, bool mixed, bool f0copy, long long cap)
 {
     char* p = static_cast<char*>(block);
     for (int d = 0; d < 3; d++) S.pos[d] = carve<double>(p, cap);
@@ -129,6 +129,7 @@ void assign_persistent(DevState& S, void* block, int NS, bool mixed, long long c
     if (mixed) {
         for (int d = 0; d < 3; d++) S.vhat32[d] = carve<float>(p, cap);
         for (int s = 0; s < 2; s++) S.N32[s] = carve<float>(p, cap);
+        if (f0copy) S.f032 = carve<float>(p, (long long)NS * cap);
     }
     S.cap = cap;
 }
@@ -177,9 +178,10 @@ int ensure_capacity(emu_context* ctx, long long n)
     // 16-byte aligned block that bulk copies may read in full
     const long long cap = (std::max<long long>(n, 1) + 127) / 128 * 128;
     for (int i = 0; i < 2; i++) {
-        CU(emu_ctx::dev_malloc(&ctx->pblock[i], persistent_bytes(ctx->NS, ctx->mixed, cap)));
+        CU(emu_ctx::dev_malloc(&ctx->pblock[i],
+                               persistent_bytes(ctx->NS, ctx->mixed, emu::mixed_f0_copy(ctx->P), cap)));
         ctx->S[i] = DevState();
-        assign_persistent(ctx->S[i], ctx->pblock[i], ctx->NS, ctx->mixed, cap);
+        assign_persistent(ctx->S[i], ctx->pblock[i], ctx->NS, ctx->mixed, emu::mixed_f0_copy(ctx->P), cap);
     }
     CU(emu_ctx::dev_malloc(&ctx->tblock, transient_bytes(ctx->NS, ctx->mixed, cap)));
     for (int i = 0; i < 2; i++) assign_transient(ctx->S[i], ctx->tblock, ctx->NS, ctx->mixed, cap);

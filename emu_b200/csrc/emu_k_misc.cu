@@ -222,8 +222,7 @@ void launch_ctl_m4(StepCtl* ctl, int nsteps, cudaStream_t st)
 
 void launch_mixed_shadow(int nf, const DevState& S, cudaStream_t st)
 {
-    (void)nf;
-    k_mixed_shadow<<<grid_for(S.n), kBlock, 0, st>>>(S);
+    k_mixed_shadow<<<grid_for(S.n), kBlock, 0, st>>>(S, 2 * nf * nf);
 }
 
 void launch_flush(double* buf, long long n, cudaStream_t st)

@@ -9,6 +9,7 @@
 //   fs, acc      fused RK4: stage state and running RK sum         FP64
 //   kgen         unfused integrators: one RHS per stage            FP64
 //   k32, ksum32  mixed RK4: previous stage RHS and weighted sum    FP32
+//   f032         mixed, 1D TSC: f0 rounded to FP32 (all stages 1-3 read)  FP32
 //   vhat32[3], N32[2]  mixed copies of the static fields           FP32
 //   id           load index of each particle                       int64
 // Meshes are cell-major: mesh[cell*ND + q] with q in GIdx order minus 3
@@ -25,6 +26,21 @@ namespace emu {
 
 // kernel parameters from the run parameters (emu_capi.cu)
 void make_devparams(const emu_params& p, DevParams& P);
+
+// Mixed stages 1-3 read the step-start state only rounded to FP32.  With 1D
+// TSC stencils (the 1,1,3 stencil widths) they read an FP32 copy of it, kept
+// by stage 4: half the bytes.  In 3D, where stage 4 stores a re-sorted state
+// every step, the copy's scattered stores cost more than the reads save
+// (C5: 26.30 -> 27.19 ms per step; C3: 0.275 -> 0.266 ms).
+template <int WX, int WY, int WZ>
+__host__ __device__ constexpr bool mixed_f0_copy_w()
+{
+    return WX == 1 && WY == 1 && WZ == 3;
+}
+inline bool mixed_f0_copy(const DevParams& P)
+{
+    return P.w[0] == 1 && P.w[1] == 1 && P.w[2] == 3;
+}
 
 struct DevState {
     long long n = 0, cap = 0;
@@ -43,6 +59,10 @@ struct DevState {
     float* ksum32 = nullptr;
     float* vhat32[3] = {};
     float* N32[2] = {};
+    // mixed path with 1D TSC stencils (mixed_f0_copy): f0 rounded to FP32,
+    // kept with f0 by every kernel that writes f0 (stages 1-3 form their FP32
+    // stage state from it); null otherwise
+    float* f032 = nullptr;
     long long* id = nullptr;
     // slot of each particle in its CTA's key-ranked deposit order (a
     // permutation of each 128-particle tile's active slots): the rank the

@@ -1177,6 +1177,8 @@ __global__ void __launch_bounds__(kBlock) k_renorm(DevParams P, DevState S, Step
     stt |= renormalize<NF>(f + NH, S.Ll[1][p], P.maxError);
     report_bad(ctl, stt, S.id[p]);
     store_state<NF>(S.f0, S.cap, p, f);
+    if (S.f032)
+        for (int c = 0; c < NS; c++) S.f032[c * S.cap + p] = (float)f[c];
 }
 
 // compute_dt for host-driven calls and the initial dt of a run
@@ -1482,6 +1484,8 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     constexpr int NH = NF * NF, NS = 2 * NH;
     constexpr int s = SG;
     constexpr bool PRELOAD = NF == 2 && SWt::MX * SWt::MY * SWt::MZ <= 3;
+    // stages 1-3 read the FP32 copy of the step-start state (mixed_f0_copy)
+    constexpr bool F32C = mixed_f0_copy_w<WX, WY, WZ>() && s < 4;
     // without the register preload, the CTA's slices of f0, k32 and ksum32
     // are staged in shared memory by bulk copies (the record area of the
     // deposit, written only after the state is consumed)
@@ -1505,7 +1509,10 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 sc_static_fields(P, S, D, p, q, pq, L2);
                 for (int d = 0; d < 3; d++) D.pos[d][q] = S.pos[d][p];
                 D.time[q] = S.time[p];
-                for (int c = 0; c < 2 * NF * NF; c++) D.f0[c * D.cap + q] = S.f0[c * S.cap + p];
+                for (int c = 0; c < 2 * NF * NF; c++) {
+                    D.f0[c * D.cap + q] = S.f0[c * S.cap + p];
+                    if (D.f032) D.f032[c * D.cap + q] = S.f032[c * S.cap + p];
+                }
             }
         }
         return;
@@ -1524,6 +1531,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     __shared__ MeshBox mbox;
     float* const mtile = reinterpret_cast<float*>(tile_smem + mixed_mesh_tile_offset<NF, WX, WY, WZ>());
     double* const sf0 = reinterpret_cast<double*>(tile_smem);        // [NS][kBlock]
+    float* const sf32 = reinterpret_cast<float*>(tile_smem);         // [NS][kBlock] (F32C)
     float* const sk = reinterpret_cast<float*>(sf0 + NS * kBlock);   // [NS][kBlock]
     float* const sks = sk + NS * kBlock;                             // [NS][kBlock]
     double* const s4 = reinterpret_cast<double*>(sks + NS * kBlock); // stage 4: time, pup[4], L[2] x kBlock
@@ -1538,11 +1546,15 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         if (t < 32) {
             if (t == 0) {
                 mbar_init(&stage_bar, 1);
-                mbar_expect_tx(&stage_bar, NS * kBlock * 8 + NKS * kBlock * 4 + (s == 4 ? 7 * kBlock * 8 : 0));
+                mbar_expect_tx(&stage_bar, NS * kBlock * (F32C ? 4 : 8) + NKS * kBlock * 4 + (s == 4 ? 7 * kBlock * 8 : 0));
                 if constexpr (MTILE) mbar_init(&mesh_bar, 1);
             }
             __syncwarp();
-            for (int c = t; c < NS; c += 32) bulk_g2s(sf0 + c * kBlock, S.f0 + c * cap + p0, kBlock * 8, &stage_bar);
+            // (F32C: the FP32 copy, in the first half of the FP64 slices' area)
+            for (int c = t; c < NS; c += 32) {
+                if (F32C) bulk_g2s(sf32 + c * kBlock, S.f032 + c * cap + p0, kBlock * 4, &stage_bar);
+                else bulk_g2s(sf0 + c * kBlock, S.f0 + c * cap + p0, kBlock * 8, &stage_bar);
+            }
             // stage 4's time, momentum and SU(n) lengths (written only by
             // the previous step too)
             if (s == 4 && t < 7) {
@@ -1585,7 +1597,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
         }
         if constexpr (PRELOAD) {
 #pragma unroll
-            for (int c = 0; c < NS; c++) y0a[c] = __ldcg(S.f0 + c * cap + p);
+            for (int c = 0; c < NS; c++) y0a[c] = F32C ? (double)__ldcg(S.f032 + c * cap + p) : __ldcg(S.f0 + c * cap + p);
         }
         make_stencil<float>(P, x, y, z, st);
     }
@@ -1713,7 +1725,9 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
             if (!live) break;
             // the stage state Y_s = y0 + aw K_{s-1} only enters the FP32
             // commutator and (stages 1-3) the FP32 deposit: formed in FP32
-            // from the FP64 step-start state; stage 4's update below is FP64
+            // from the step-start state rounded to FP32 (with 1D stencils
+            // stages 1-3 read only its FP32 copy); stage 4's update below is
+            // FP64
             double y0[NH];
             float y0f[NH], f32[NH];
 #pragma unroll
@@ -1723,7 +1737,7 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                     y0[e] = y0a[sp * NH + e];
                     k = ka[sp * NH + e];
                 } else {
-                    y0[e] = sf0[(sp * NH + e) * kBlock + t];
+                    y0[e] = F32C ? (double)sf32[(sp * NH + e) * kBlock + t] : sf0[(sp * NH + e) * kBlock + t];
                     k = s > 1 ? sk[(sp * NH + e) * kBlock + t] : 0.f;
                 }
                 y0f[e] = (float)y0[e];
@@ -1781,9 +1795,16 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 stt |= renormalize<NF>(fn, PRELOAD ? Lsp[sp] : s4[(5 + sp) * kBlock + t], P.maxError);
 #pragma unroll
                 for (int e = 0; e < NH; e++) {
-                    if constexpr (SC) D.f0[(sp * NH + e) * cap + qsc] = fn[e];
-                    else S.f0[(sp * NH + e) * cap + p] = fn[e];
-                    fN[sp * NH + e] = (float)fn[e] * Ns;
+                    const float f32n = (float)fn[e];
+                    constexpr bool C32 = mixed_f0_copy_w<WX, WY, WZ>();
+                    if constexpr (SC) {
+                        D.f0[(sp * NH + e) * cap + qsc] = fn[e];
+                        if constexpr (C32) D.f032[(sp * NH + e) * cap + qsc] = f32n;
+                    } else {
+                        S.f0[(sp * NH + e) * cap + p] = fn[e];
+                        if constexpr (C32) S.f032[(sp * NH + e) * cap + p] = f32n;
+                    }
+                    fN[sp * NH + e] = f32n * Ns;
                 }
             }
         }
@@ -1971,6 +1992,8 @@ __global__ void k_gather_state(DevState src, DevState dst, const unsigned* __res
     if (mixed) {
         for (int d = 0; d < 3; d++) dst.vhat32[d][i] = src.vhat32[d][j];
         for (int sp = 0; sp < 2; sp++) dst.N32[sp][i] = src.N32[sp][j];
+        if (dst.f032)
+            for (int c = 0; c < NS; c++) dst.f032[c * dst.cap + i] = src.f032[c * src.cap + j];
     }
 }
 
@@ -2029,8 +2052,12 @@ __global__ void __launch_bounds__(kBlock) k_gather_deposit(DevParams P, DevState
         for (int c = 0; c < NS; c++) {
             const double f = src.f0[c * src.cap + j];
             dst.f0[c * dst.cap + i] = f;
-            if constexpr (MIXED) fN[c] = (float)f * N32[c / NH];
-            else fN[c] = f * Nn[c / NH];
+            if constexpr (MIXED) {
+                if (dst.f032) dst.f032[c * dst.cap + i] = (float)f;
+                fN[c] = (float)f * N32[c / NH];
+            } else {
+                fN[c] = f * Nn[c / NH];
+            }
         }
         make_stencil<R>(P, x[0], x[1], x[2], st);
     }
@@ -2077,12 +2104,14 @@ __global__ void __launch_bounds__(kBlock) k_deposit_comb(DevParams P, DevState S
                                                                     QuantConvG{P});
 }
 
-__global__ void k_mixed_shadow(DevState S)
+__global__ void k_mixed_shadow(DevState S, int ns)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= S.n) return;
     for (int d = 0; d < 3; d++) S.vhat32[d][i] = (float)S.vhat[d][i];
     for (int sp = 0; sp < 2; sp++) S.N32[sp][i] = (float)S.Nn[sp][i];
+    if (S.f032)
+        for (int c = 0; c < ns; c++) S.f032[c * S.cap + i] = (float)S.f0[c * S.cap + i];
 }
 
 template <int NF>
