@@ -535,6 +535,7 @@ def run_emu(args):
                "sample": "%d RK4 steps of %s, FP64, %.1f s" % (done, sdesc, el)}
 
     kernels_per_step = 1 if coop else (8 if mixed else 4)
+    widths = [1 if c <= 1 else (3 if p.shape_order >= 2 else (2 if p.shape_order == 1 else 1)) for c in p.ncell]
     resorts = (args.steps // eff_resort) if eff_resort > 0 else 0
     key_bits = int(np.ceil(np.log2(max(int(np.prod(list(p.ncell))) + 1, 2))))
     out = {
@@ -565,13 +566,14 @@ def run_emu(args):
         "e2e": e2e,
         "cpu_baseline": cpu,
         # per step: the step kernels (+ the L2 flush for small states); per
-        # re-sort: keys, radix sort (histogram, scan, one pass per 8 key
-        # bits) and the gather (FP64), or the inversion of the permutation
-        # and the deposit of the sorted state (mixed: stage 4 stores in
-        # cell order); per emu_evolve_steps call of the mixed path: the
-        # stage-4 mesh control
+        # re-sort: radix sort (histogram, scan, one pass per 8 key bits),
+        # the keys (a kernel of their own unless stage 3 of a mixed step
+        # with 3D stencils stores them) and the gather (FP64), or the
+        # inversion of the permutation and the deposit of the sorted state
+        # (mixed: stage 4 stores the state in cell order); per
+        # emu_evolve_steps call of the mixed path: the stage-4 mesh control
         "gpu_launches": args.steps * kernels_per_step + (args.steps if flush is not None else 0) +
-                        resorts * (4 + (key_bits + 7) // 8 + (1 if mixed else 0)) +
+                        resorts * (4 + (key_bits + 7) // 8 + (1 if mixed and widths == [1, 1, 3] else 0)) +
                         ((args.steps if flush is not None else 1) if mixed else 0),
         "clocks": clocks,
         "wall_s": wall,

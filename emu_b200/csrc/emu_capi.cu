@@ -224,16 +224,17 @@ int sort_perm(emu_context* ctx, long long n, cudaStream_t st)
 }
 int sort_perm(emu_context* ctx, long long n) { return sort_perm(ctx, n, ctx->stream); }
 
-// The mixed path's re-sort after a step, around stage 4: keys of the
-// positions after the step and their sort before it (the inverse
-// permutation in idx), the deposit of the re-sorted state after it.  The
-// next step's first mesh is zeroed here too: once the run has ended the
-// finalize kernel does not, and the unchanged state is deposited again.
+// The mixed path's re-sort after a step, around stage 4: the keys of the
+// positions after the step (stored by stage 3 into keys and idx, or here
+// when !sc_keys_in_stage3) and their sort before it (the inverse permutation in idx), the deposit of the
+// re-sorted state after it.  The next step's first mesh is zeroed here too:
+// once the run has ended the finalize kernel does not, and the unchanged
+// state is deposited again.
 int enqueue_sc_before(emu_context* ctx, cudaStream_t st)
 {
     const DevState& S = ctx->S[ctx->cur];
     CU(cudaMemsetAsync(ctx->qmesh[0], 0, sizeof(long long) * ctx->P.ncells * ctx->ND, st));
-    emu::launch_sc_keys(ctx->P, S, ctx->ctl, ctx->keys, ctx->idx, st);
+    if (!emu::sc_keys_in_stage3(ctx->P)) emu::launch_sc_keys(ctx->P, S, ctx->ctl, ctx->keys, ctx->idx, st);
     int r;
     if ((r = sort_perm(ctx, S.n, st))) return r;
     emu::launch_sc_invert(ctx->idx2, ctx->idx, S.n, st);
@@ -390,8 +391,11 @@ int enqueue_rk4_mixed(emu_context* ctx, cudaStream_t st, bool with_dt, bool dep4
             continue;
         }
         const bool dep = s < 4 || dep4;
+        // (stage 3 before a re-sort made by stage 4: the re-sort keys)
+        const bool keys = s == 3 && !dep4 && emu::sc_keys_in_stage3(ctx->P);
         emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr, ctx->qmesh[1],
-                                    m4_target(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st);
+                                    m4_target(ctx), ctx->ctl, (s == 4 && with_dt) ? emu::DT_ADVANCE : -1, st, nullptr,
+                                    nullptr, keys ? ctx->keys : nullptr, keys ? ctx->idx : nullptr);
         if (dep && (r = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return r;
         a = b;
     }
@@ -1085,7 +1089,8 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
     int k = 0;
     auto rec = [&](int i) { return cudaEventRecord(ev[i], st); };
     // (mixed: the re-sort made around stage 4, timed as one entry after the
-    // stages: its keys and sort before stage 4 plus its deposit after it)
+    // stages: its keys (unless stage 3 stores them) and sort before stage 4
+    // plus its deposit after it)
     const bool sc = ctx->mixed && resort_due;
     if (ctx->mixed) {
         int a = 0;
@@ -1117,8 +1122,10 @@ int emu_profile_step(emu_context* ctx, float* kernel_ms, int max_kernels, int* n
             }
             const bool dep = s < 4 || !resort_due;
             rec(2 * k);
+            const bool keys = s == 3 && sc && emu::sc_keys_in_stage3(ctx->P);
             emu::launch_rk4_stage_mixed(ctx->nf, ctx->P, S, s, ctx->gmesh, dep ? ctx->qmesh[b] : nullptr,
-                                        ctx->qmesh[1], m4_target(ctx), ctx->ctl, s == 4 ? emu::DT_ADVANCE : -1, st);
+                                        ctx->qmesh[1], m4_target(ctx), ctx->ctl, s == 4 ? emu::DT_ADVANCE : -1, st,
+                                        nullptr, nullptr, keys ? ctx->keys : nullptr, keys ? ctx->idx : nullptr);
             rec(2 * k + 1);
             k++;
             if (dep && (rr = emu_ctx::reduce_mesh(ctx, ctx->qmesh[b], true, st))) return rr;

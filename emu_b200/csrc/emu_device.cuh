@@ -13,6 +13,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace emu {
@@ -508,6 +509,15 @@ __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, 
     if (cur >= 0) flush(cur);
 }
 
+// The diagonal slots a combined deposit may sum in the same walk over its
+// records (DiagOut), or none (NoDiag).
+struct NoDiag {};
+template <class T, class Conv>
+struct DiagOut {
+    T* diag;     // diag[cell * kDiagSlots + c]
+    Conv conv;   // per-species fixed-point conversion
+};
+
 // Combined deposit of the mixed path (FP32 records): per cell the Comb<NF>
 // values G[d][j] = sum w v_d c_j (v_0 = 1), which is all a stage's
 // interpolation reads.  Records hold the particle's NV values c_j; thread
@@ -515,10 +525,16 @@ __device__ __forceinline__ void tile_deposit_pairs(const DevParams& P, T* mesh, 
 // them to mesh[cell * NG + q].  Three flavors: NG = 32, each stream is one
 // warp (no divergence between streams).  The weights are read as 16-byte
 // vectors, two pairs of the packed FMA each.
-template <int NF, int BLOCK, int NTILE, class SWt, class T, class Conv>
+// With a DiagOut (27-cell stencils, three flavors): lane k < 27 of each
+// stream also sums the 2 NF diagonal values of the records (at SP + NV,
+// combined layout) with stencil weight k, as tile_deposit_diag's lane per
+// stencil cell does (the same record ranges, runs and FP32 operations, so
+// the same int64 sums), sharing this walk's key tests and flushes.
+template <int NF, int BLOCK, int NTILE, class SWt, class T, class Conv, class DG = NoDiag>
 __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, const int* skey, const float* srec,
-                                                  int ntile, Conv conv)
+                                                  int ntile, Conv conv, DG dg = {})
 {
+    constexpr bool WITH_DIAG = !std::is_same<DG, NoDiag>::value;
     using TR = TileRec<NF, SWt, float>;
     using C = Comb<NF>;
     constexpr int NS = 2 * NF * NF, NV = C::NV, NG = C::NG, RW = TR::RW, SP = TR::SP, S = TR::S;
@@ -533,7 +549,12 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
     const int d = q / NV, j = q % NV;
     const int coff = SP + j;
     const int voff = SP + NS + (d > 0 ? d - 1 : 0);
+    static_assert(!WITH_DIAG || (S == 27 && NG == 32 && NF == 3), "diagonal slots: a lane per stencil cell");
+    // (WITH_DIAG: this lane's stencil cell)
+    const int dk = q / 9, dj = (q / 3) % 3, di = q % 3;
+    const bool don = WITH_DIAG && q < S && SWt::on(P, di, dj, dk);
     float2 acc[NP];
+    float2 dacc[WITH_DIAG ? NF : 1];
     auto flush = [&](int key) {
         const int bx = key % P.n[0];
         const int by = (key / P.n[0]) % P.n[1];
@@ -549,6 +570,24 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
                     const float a = (k & 1) ? acc[k / 2].y : acc[k / 2].x;
                     atomic_add_mesh(&mesh[cell_of(P, bx, by, bz, ii, jj, kk) * NG + q], conv(a, 0));
                 }
+        if constexpr (WITH_DIAG) {
+            if (don) {
+                T* g = dg.diag + cell_of(P, bx, by, bz, di, dj, dk) * kDiagSlots;
+#pragma unroll
+                for (int m = 0; m < NF; m++) {
+                    atomic_add_mesh(g + 2 * m, dg.conv(dacc[m].x, (2 * m) / NF));
+                    atomic_add_mesh(g + 2 * m + 1, dg.conv(dacc[m].y, (2 * m + 1) / NF));
+                }
+            }
+        }
+    };
+    auto zero = [&]() {
+#pragma unroll
+        for (int k = 0; k < NP; k++) acc[k] = f2(0.f, 0.f);
+        if constexpr (WITH_DIAG) {
+#pragma unroll
+            for (int m = 0; m < NF; m++) dacc[m] = f2(0.f, 0.f);
+        }
     };
     auto add_one = [&](int i) {
         const float* r = srec + i * RW;
@@ -562,13 +601,21 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
             acc[k] = __ffma2_rn(f2(w.x, w.y), qq, acc[k]);
             if (k + 1 < NP) acc[k + 1] = __ffma2_rn(f2(w.z, w.w), qq, acc[k + 1]);
         }
+        if constexpr (WITH_DIAG) {
+            const float wt = q < S ? r[q] : 0.f;
+            const float2 ww = f2(wt, wt);
+#pragma unroll
+            for (int m = 0; m < NF; m++) {
+                const float2 x = reinterpret_cast<const float2*>(r + SP + NV)[m];
+                dacc[m] = __ffma2_rn(x, ww, dacc[m]);
+            }
+        }
     };
     // (four at a time: measured 2 % faster than two on C5's stage kernels)
     constexpr int BATCH = 4;
     const int i1 = min((stream + 1) * CH, ntile);
     int cur = -1;
-#pragma unroll
-    for (int k = 0; k < NP; k++) acc[k] = f2(0.f, 0.f);
+    zero();
     for (int i = stream * CH; i < i1; i++) {
         // BATCH records of the current run in one go: their loads are
         // independent and issue together (the stream's keys are sorted,
@@ -587,8 +634,7 @@ __device__ __forceinline__ void tile_deposit_comb(const DevParams& P, T* mesh, c
         const int key = skey[i];
         if (key != cur) {
             if (cur >= 0) flush(cur);
-#pragma unroll
-            for (int k = 0; k < NP; k++) acc[k] = f2(0.f, 0.f);
+            zero();
             cur = key;
         }
         if (key < 0) continue;

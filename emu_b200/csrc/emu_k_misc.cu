@@ -15,7 +15,8 @@ namespace emu {
                                           double*, cudaStream_t);                                                \
     extern template void launch_rk4_stage_mixed_t<NF>(const DevParams&, const DevState&, int, const float*,      \
                                                       long long*, const long long*, long long*, StepCtl*, int,   \
-                                                      cudaStream_t, const DevState*, const unsigned*);           \
+                                                      cudaStream_t, const DevState*, const unsigned*, unsigned*, \
+                                                      unsigned*);                                                \
     extern template void launch_deposit_comb_t<NF>(const DevParams&, const DevState&, long long*, cudaStream_t);  \
     extern template void launch_deposit_q_t<NF>(const DevParams&, const DevState&, const double*, long long*,    \
                                                 cudaStream_t);                                                   \
@@ -132,10 +133,19 @@ cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, 
 
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
                             long long* qmesh_out, const long long* qmesh_dt, long long* qmesh_m4, StepCtl* ctl,
-                            int dt_mode, cudaStream_t st, const DevState* D, const unsigned* inv)
+                            int dt_mode, cudaStream_t st, const DevState* D, const unsigned* inv, unsigned* kout,
+                            unsigned* iout)
 {
-    if (nf == 2) launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st, D, inv);
-    else launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st, D, inv);
+    if (nf == 2)
+        launch_rk4_stage_mixed_t<2>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st, D, inv, kout, iout);
+    else
+        launch_rk4_stage_mixed_t<3>(P, S, s, gmesh, qmesh_out, qmesh_dt, qmesh_m4, ctl, dt_mode, st, D, inv, kout, iout);
+}
+
+void launch_sc_keys(const DevParams& P, const DevState& S, const StepCtl* ctl, unsigned* keys, unsigned* idx,
+                    cudaStream_t st)
+{
+    k_sc_keys<<<grid_for(S.n), kBlock, 0, st>>>(P, S, ctl, keys, idx);
 }
 
 void launch_deposit_comb(int nf, const DevParams& P, const DevState& S, long long* qmesh, cudaStream_t st)
@@ -144,11 +154,6 @@ void launch_deposit_comb(int nf, const DevParams& P, const DevState& S, long lon
     else launch_deposit_comb_t<3>(P, S, qmesh, st);
 }
 
-void launch_sc_keys(const DevParams& P, const DevState& S, const StepCtl* ctl, unsigned* keys, unsigned* idx,
-                    cudaStream_t st)
-{
-    k_sc_keys<<<grid_for(S.n), kBlock, 0, st>>>(P, S, ctl, keys, idx);
-}
 
 void launch_sc_invert(const unsigned* perm, unsigned* inv, long long n, cudaStream_t st)
 {

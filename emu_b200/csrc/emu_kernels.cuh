@@ -42,6 +42,22 @@ inline bool mixed_f0_copy(const DevParams& P)
     return P.w[0] == 1 && P.w[1] == 1 && P.w[2] == 3;
 }
 
+// The keys of the re-sort made by stage 4 (the stencil keys after the step)
+// are stored by stage 3 of that step, except with 1D TSC stencils (a
+// re-sort every 16 steps), where a kernel of their own computes them before
+// the sort and stage 3 keeps no code for them (C5: 26.30 -> 25.89 ms per
+// step with the fused diagonal slots; C3 0.2655 -> 0.2692 ms when its stage
+// 3 held the key path too).
+template <int WX, int WY, int WZ>
+__host__ __device__ constexpr bool sc_keys_in_stage3_w()
+{
+    return !(WX == 1 && WY == 1 && WZ == 3);
+}
+inline bool sc_keys_in_stage3(const DevParams& P)
+{
+    return !(P.w[0] == 1 && P.w[1] == 1 && P.w[2] == 3);
+}
+
 struct DevState {
     long long n = 0, cap = 0;
     double* pos[3] = {};
@@ -132,16 +148,17 @@ cudaError_t launch_rk4_step_coop(int nf, const DevParams& P, const DevState& S, 
 // qmesh_m4: stage 3's target for the full stage-4 mesh (DevParams::m4_reduced)
 // D, inv (stage 4 only): the stage that makes the cell re-sort following the
 // step: particle p's new state and unchanged fields go to slot inv[p] of D
-// (launch_sc_keys, the radix sort and launch_sc_invert before it; the
-// combined deposit of D, launch_deposit_comb, after it).
+// (the radix sort of the keys and launch_sc_invert before it; the combined
+// deposit of D, launch_deposit_comb, after it).  kout, iout (stage 3 of a
+// step followed by such a re-sort): each particle's stencil key after the
+// step and the identity index, which that sort orders.
 void launch_rk4_stage_mixed(int nf, const DevParams& P, const DevState& S, int s, const float* gmesh,
                             long long* qmesh_out, const long long* qmesh_dt, long long* qmesh_m4, StepCtl* ctl,
                             int dt_mode, cudaStream_t st, const DevState* D = nullptr,
-                            const unsigned* inv = nullptr);
+                            const unsigned* inv = nullptr, unsigned* kout = nullptr, unsigned* iout = nullptr);
 // the combined deposit of a cell-sorted mixed state into qmesh (zeroed)
 void launch_deposit_comb(int nf, const DevParams& P, const DevState& S, long long* qmesh, cudaStream_t st);
-// keys of the positions after the step (the stage-4 push; unchanged once the
-// run has ended) and the identity index
+// the same keys in a kernel of their own (when !sc_keys_in_stage3)
 void launch_sc_keys(const DevParams& P, const DevState& S, const StepCtl* ctl, unsigned* keys, unsigned* idx,
                     cudaStream_t st);
 // inv[perm[i]] = i

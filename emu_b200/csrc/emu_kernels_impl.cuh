@@ -552,12 +552,14 @@ __device__ __forceinline__ bool distinct_key_rank(int key, int* scratch, int& sl
 // COMB: the mixed path's combined deposit (fN holds the Comb<NF> values;
 // NREC > NV: further values the records carry for a later pass)
 // given_slot >= 0 (in every thread, or in none): the record slots are given
-// (a rank made earlier for the same keys) and no ranking is done.  Returns
-// the thread's slot.
-template <int NF, class SWt, class R, class T, class Conv, bool COMB = false, int NREC = Comb<NF>::NV>
+// (a rank made earlier for the same keys) and no ranking is done.
+// dg (COMB): the diagonal slots summed in the same walk (tile_deposit_comb).
+// Returns the thread's slot.
+template <int NF, class SWt, class R, class T, class Conv, bool COMB = false, int NREC = Comb<NF>::NV,
+          class DG = NoDiag>
 __device__ __forceinline__ int tile_deposit_block(const DevParams& P, T* mesh, bool active, const Stencil<R>& st,
                                                   const R* fN, R vx, R vy, R vz, Conv conv, bool sort_keys = false,
-                                                  int given_slot = -1)
+                                                  int given_slot = -1, DG dg = {})
 {
     using Sort = cub::BlockRadixSort<unsigned, kBlock, 1, int>;
     static_assert(sizeof(typename Sort::TempStorage) <= kBlock * TileRec<NF, SWt, R>::RW * sizeof(R),
@@ -590,7 +592,7 @@ __device__ __forceinline__ int tile_deposit_block(const DevParams& P, T* mesh, b
     if constexpr (COMB) {
         tile_record<NF, SWt, R, NREC>(srec, skey, slot, key, fN, vx, vy, vz, st);
         __syncthreads();
-        tile_deposit_comb<NF, kBlock, kBlock, SWt, T>(P, mesh, skey, srec, kBlock, conv);
+        tile_deposit_comb<NF, kBlock, kBlock, SWt, T>(P, mesh, skey, srec, kBlock, conv, dg);
     } else {
         tile_record<NF, SWt, R>(srec, skey, slot, key, fN, vx, vy, vz, st);
         __syncthreads();
@@ -1411,19 +1413,17 @@ __host__ __device__ constexpr int mixed_mesh_tile_offset()
            (mixed_mesh_tile<NF, WX, WY, WZ>() ? kMeshTileCells * Comb<NF>::NG * 4 : 0);
 }
 
-// Keys of the cell re-sort that the next stage 4 scatters into: every
-// particle's stencil key after the step (the stage-4 push; none once the
-// run has ended), with the identity index, for the radix sort.
-__global__ void k_sc_keys(DevParams P, DevState S, const StepCtl* __restrict__ ctl, unsigned* __restrict__ keys,
-                          unsigned* __restrict__ idx)
+// Key of the cell re-sort that the next stage 4 scatters into, stored by
+// stage 3 of a step followed by a re-sort: particle p's stencil key after
+// the step (the stage-4 push of its momentum with the step's dt; the key of
+// the unchanged position once the run has ended), with the identity index,
+// for the radix sort.
+__device__ __forceinline__ void sc_key(const DevParams& P, const DevState& S, long long p, double dt, bool push,
+                                       unsigned* keys, unsigned* idx)
 {
-    const int done = __ldcg(&ctl->done);
-    const double dt = __ldcg(&ctl->dt);
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= S.n) return;
-    double xn[3] = {S.pos[0][p], S.pos[1][p], S.pos[2][p]};
-    if (!done) {
-        const double pq[4] = {S.pup[0][p], S.pup[1][p], S.pup[2][p], S.pup[3][p]};
+    double xn[3] = {__ldcg(S.pos[0] + p), __ldcg(S.pos[1] + p), __ldcg(S.pos[2] + p)};
+    if (push) {
+        const double pq[4] = {__ldcg(S.pup[0] + p), __ldcg(S.pup[1] + p), __ldcg(S.pup[2] + p), __ldcg(S.pup[3] + p)};
         double tn = 0.0;
         rk4_push(P, dt, pq, xn, tn);
     }
@@ -1431,6 +1431,16 @@ __global__ void k_sc_keys(DevParams P, DevState S, const StepCtl* __restrict__ c
     make_stencil<double>(P, xn[0], xn[1], xn[2], st);
     keys[p] = (unsigned)stencil_key(P, st.b);
     idx[p] = (unsigned)p;
+}
+
+// the same keys before the sort, when stage 3 does not store them
+__global__ void k_sc_keys(DevParams P, DevState S, const StepCtl* __restrict__ ctl, unsigned* __restrict__ keys,
+                          unsigned* __restrict__ idx)
+{
+    const int done = __ldcg(&ctl->done);
+    const double dt = __ldcg(&ctl->dt);
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < S.n) sc_key(P, S, p, dt, !done, keys, idx);
 }
 
 // inverse of the sort's permutation: particle perm[i] goes to slot i
@@ -1468,7 +1478,8 @@ __device__ __forceinline__ void sc_static_fields(const DevParams& P, const DevSt
 // SC (stage 4 before a re-sort): the new state and every unchanged field of
 // particle p go to slot inv[p] of D, the other particle buffer, in the new
 // cell order (the re-sort's gather, made by the stores of this stage; its
-// keys and sort ran before it, from the same push); D's deposit follows.
+// keys, stored by stage 3 into kout/iout, and their sort ran before it,
+// from the same push); D's deposit follows.
 template <int NF, int WX, int WY, int WZ, int SG, bool SC = false>
 // (1D: 5 CTAs per SM at 96 registers beat 4 at 128 despite the spills)
 __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(DevParams P, DevState S,
@@ -1477,7 +1488,9 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                                                             const long long* __restrict__ qdt,
                                                             long long* __restrict__ qm4, StepCtl* ctl,
                                                             int dt_mode, DevState D,
-                                                            const unsigned* __restrict__ inv)
+                                                            const unsigned* __restrict__ inv,
+                                                            unsigned* __restrict__ kout,
+                                                            unsigned* __restrict__ iout)
 {
     using H = Herm<NF>;
     using SWt = SW<WX, WY, WZ>;
@@ -1496,6 +1509,10 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
     const int done = __ldcg(&ctl->done);
     const double dt = __ldcg(&ctl->dt);   // both control loads in one round trip
     if (done) {
+        if constexpr (SG == 3 && sc_keys_in_stage3_w<WX, WY, WZ>()) {
+            const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (kout && p < S.n) sc_key(P, S, p, dt, false, kout, iout);
+        }
         if constexpr (SC) {
             // after the run's end the re-sort still moves the unchanged
             // state (its keys were those of the unchanged positions)
@@ -1600,6 +1617,10 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
             for (int c = 0; c < NS; c++) y0a[c] = F32C ? (double)__ldcg(S.f032 + c * cap + p) : __ldcg(S.f0 + c * cap + p);
         }
         make_stencil<float>(P, x, y, z, st);
+        // (a re-sort follows the step: its keys, from fields no kernel of
+        // the step writes)
+        if constexpr (SG == 3 && sc_keys_in_stage3_w<WX, WY, WZ>())
+            if (kout) sc_key(P, S, p, dt, true, kout, iout);
     }
     if constexpr (MTILE) {
         // the CTA's smallest and largest stencil key
@@ -1859,12 +1880,21 @@ __global__ void __launch_bounds__(kBlock, WX == 1 ? 5 : 4) k_rk4_stage_mixed(Dev
                 cN[NV + i] = fN[H::re(i, i)];
                 cN[NV + NF + i] = fN[NH + H::re(i, i)];
             }
-            const int sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true, NV + 2 * NF>(
-                P, qout, live, st, cN, vx, vy, vz, QuantConvG{P}, false, given);
-            // (the records the deposit above has read, still in place)
-            tile_deposit_diag<NF, kBlock, kBlock, SWt, long long>(
-                P, qout + P.ncells * (8 * NH), reinterpret_cast<const int*>(tile_smem),
-                reinterpret_cast<const float*>(tile_smem + kBlock * 8), kBlock, true, QuantConv{P});
+            long long* const qdiag = qout + P.ncells * (8 * NH);
+            int sl;
+            if constexpr (NF == 3 && SWt::MX * SWt::MY * SWt::MZ == 27) {
+                // (27-cell stencils: the diagonal slots in the same walk)
+                sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true, NV + 2 * NF>(
+                    P, qout, live, st, cN, vx, vy, vz, QuantConvG{P}, false, given,
+                    DiagOut<long long, QuantConv>{qdiag, QuantConv{P}});
+            } else {
+                sl = tile_deposit_block<NF, SWt, float, long long, QuantConvG, true, NV + 2 * NF>(
+                    P, qout, live, st, cN, vx, vy, vz, QuantConvG{P}, false, given);
+                // (the records the deposit above has read, still in place)
+                tile_deposit_diag<NF, kBlock, kBlock, SWt, long long>(
+                    P, qdiag, reinterpret_cast<const int*>(tile_smem),
+                    reinterpret_cast<const float*>(tile_smem + kBlock * 8), kBlock, true, QuantConv{P});
+            }
             const bool full = m4_full_step(ctl);   // uniform over the grid
             if (full) {
                 __syncthreads();   // every record has been read
@@ -2333,14 +2363,15 @@ void launch_rhs_t(const DevParams& P, const DevState& S, const double* f, const 
 template <int NF>
 void launch_rk4_stage_mixed_t(const DevParams& P, const DevState& S, int s, const float* gmesh, long long* qout,
                               const long long* qdt, long long* qm4, StepCtl* ctl, int dt_mode, cudaStream_t st,
-                              const DevState* D, const unsigned* inv)
+                              const DevState* D, const unsigned* inv, unsigned* kout, unsigned* iout)
 {
     EMU_W_DISPATCH(P, {
         constexpr int bytes = mixed_stage_smem_bytes<NF, WXv, WYv, WZv>();
         const DevState& Dv = D ? *D : S;
         auto go = [&](auto kern) {
             smem_optin(kern, bytes);
-            launch_pdl(kern, grid_for(S.n), kBlock, bytes, st, P, S, gmesh, qout, qdt, qm4, ctl, dt_mode, Dv, inv);
+            launch_pdl(kern, grid_for(S.n), kBlock, bytes, st, P, S, gmesh, qout, qdt, qm4, ctl, dt_mode, Dv, inv,
+                       kout, iout);
         };
         if (s == 1) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 1>);
         else if (s == 2) go(k_rk4_stage_mixed<NF, WXv, WYv, WZv, 2>);
